@@ -1,0 +1,198 @@
+/*
+ * mmnb.h — C ABI of libmmnb, the sm_100a implementation of msim's nonbonded
+ * force path: real-space Ewald erfc-Coulomb + Lennard-Jones over a GPU-built
+ * cell neighbour list, and the P3M / ordinary-Ewald reciprocal space.
+ *
+ * One handle is one ElecLJ potential (include/eleclj.hpp:303-397 in the
+ * reference) bound to one CUDA device and one stream.  Plain C types only:
+ * pointers, sizes and int status codes, so any FFI can bind it.
+ *
+ * What each entry point replaces in the reference:
+ *
+ *   mmnb_create / mmnb_set_params   ElecLJ::init, types_changed, set_lambda
+ *                                   (src/eleclj.cpp:140-265, 273-319, 328-580)
+ *                                   and the set-up halves of the C kernels:
+ *                                   RSpaceChebyshev_new (include/rspace.h:17),
+ *                                   p3m_new + p3m_init (include/pppm.h:12-35),
+ *                                   kspace_new (include/kspace.h:11),
+ *                                   NeighborList::NeighborList +
+ *                                   set_boundary_conditions (include/nbrlist.hpp:15-18)
+ *   mmnb_compute                    ElecLJ::add_to_energy_and_forces, i.e.
+ *                                   Potential::add_to_energy_and_forces
+ *                                   (include/pot.hpp:12, src/eleclj.cpp:785-807),
+ *                                   which runs NeighborList::coordinates_changed,
+ *                                   RSpaceEwald (include/rspace.h:19-34),
+ *                                   p3m_field (include/pppm.h:52-56) or
+ *                                   kspace_field (include/kspace.h:14-15),
+ *                                   calc_self_phi and the LJ tail
+ *   mmnb_scale                      ElecLJ::scale + p3m_scale (src/eleclj.cpp:1268-1280,
+ *                                   include/pppm.h:60)
+ *   mmnb_destroy                    ElecLJ::cleanup, p3m_delete, kspace_delete
+ *
+ * Conventions are the reference's: Angstrom, kcal/mol, charges in
+ * sqrt(kcal A / mol) (e_to_charge_unit, include/units.h:91-94); vectors are AoS
+ * double[3] (cart_t, include/cart.h:9).  Forces are ADDED to the caller's
+ * array and the energy is ADDED to *u, as Potential::add_to_energy_and_forces
+ * does; the caller zeroes them (src/mdyn.cpp:151-153).
+ *
+ * Where the reference calls die() or an assertion, these functions return a
+ * nonzero status and leave the handle usable; mmnb_last_error() explains.
+ */
+#ifndef MMNB_H
+#define MMNB_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define MMNB_OK 0
+#define MMNB_ERR_ARG 1          /* bad argument (sizes, ranges, null pointers) */
+#define MMNB_ERR_CUDA 2         /* a CUDA or cuFFT call failed */
+#define MMNB_ERR_UNSUPPORTED 3  /* option this build does not provide */
+#define MMNB_ERR_CUTOFF 4       /* rspace_cutoff > 0.49 * minimum box diameter,
+                                   or smoothing_width >= cutoff (src/eleclj.cpp:168-182) */
+#define MMNB_ERR_OVERFLOW 5     /* neighbour rows outgrew their capacity after a retry */
+#define MMNB_ERR_STATE 6        /* call out of order (e.g. compute before set_params) */
+#define MMNB_ERR_TIMEOUT 7      /* a bounded device-side wait gave up */
+#define MMNB_ERR_DEVICE 8       /* a device-side check failed (index or size out of range) */
+
+/* precision forms */
+#define MMNB_FP64 0   /* FP64 throughout; matches the reference to ~1e-12 relative */
+#define MMNB_MIXED 1  /* FP32 pair and spline math, 64-bit fixed-point force
+                         accumulation, FP64 energies, self terms and influence function */
+
+/* boundary conditions: enum bcondtype_t values (include/bcondtype.h:8) */
+#define MMNB_CUBIC 1
+#define MMNB_ORTHORHOMBIC 2
+
+/* site flags (include/rspace.h:7-8) */
+#define MMNB_SITE_HAS_Q 1
+#define MMNB_SITE_HAS_LJ 2
+
+typedef struct mmnb_handle mmnb_handle;
+
+/* ElecLJ's hot-path input fields (include/eleclj.hpp:310-328); defaults from
+   mmnb_config_init are the reference's (src/eleclj.cpp:13-40). */
+typedef struct mmnb_config {
+  int precision;                 /* MMNB_FP64 or MMNB_MIXED */
+  int bctype;                    /* MMNB_CUBIC or MMNB_ORTHORHOMBIC */
+  double box[3];                 /* edge lengths (A); cubic reads box[0] */
+  double rspace_cutoff;          /* 0 -> 0.45 * minimum diameter */
+  double smoothing_width;        /* 1 */
+  double neighbor_list_width;    /* 0 -> 0.2 rc, clipped to 0.499 d - rc */
+  double kspace_cutoff;          /* 5 (ordinary Ewald |n| cutoff) */
+  double ewald_screening;        /* -1 -> automatic; P3M needs an explicit value */
+  int use_p3m;                   /* 0 */
+  double p3m_grid_spacing;       /* 0.5 */
+  int p3m_assignment_order;      /* 3; 2..7 */
+  int p3m_alias_sum_limit;       /* 2 */
+  int p3m_ik_differentiate;      /* 0 */
+  int include_lj_correction;     /* 1 */
+  int geometric_combining_for_sigma; /* 0 */
+  int include_rspace;            /* 1 */
+  int include_kspace;            /* 1 */
+  int include_self;              /* 1 */
+  double elec_1_4_scale_factor;  /* 1 */
+  double lj_1_4_scale_factor;    /* 1 */
+  int rebuild_interval;          /* 0: rebuild on the reference's displacement
+                                    criterion (src/nbrlist.cpp:51-77); k > 0: also
+                                    force a rebuild every k-th evaluation */
+  int device;                    /* CUDA ordinal, -1 = current */
+} mmnb_config;
+
+/* Energies of the last evaluation (kcal/mol), as ElecLJ::write reports them
+   (src/eleclj.cpp:1026-1150). */
+typedef struct mmnb_energy {
+  double elec;            /* (q . phi) / 2 */
+  double lj;              /* pair LJ + tail correction */
+  double lj_correction;   /* tail alone */
+  double total;           /* elec + lj: what is added to u */
+} mmnb_energy;
+
+/* Fill *c with the reference's defaults. */
+int mmnb_config_init(mmnb_config *c);
+
+/* Create a potential for nsite sites in ngroup groups.
+   group: 2*ngroup ints, half-open site ranges [a, b) of each group; the first
+          site of a group is its anchor (src/eleclj.cpp:654-681, 778-779).
+   excl:  2*nexcl site pairs excluded from the pair sum (1-2 and 1-3 pairs,
+          src/eleclj.cpp:712-724), either order, duplicates allowed.
+   pairs14: 2*n14 site pairs for the scaled 1-4 terms; read only when a 1-4
+          scale factor differs from 1 (src/eleclj.cpp:726-747). */
+int mmnb_create(const mmnb_config *c, int nsite, int ngroup, const int *group,
+                int nexcl, const int *excl, int n14, const int *pairs14,
+                mmnb_handle **out);
+
+/* Per-site parameters: mask bits MMNB_SITE_HAS_Q / MMNB_SITE_HAS_LJ, charge
+   (internal unit), LJ sigma (A) and epsilon (kcal/mol), short-range
+   screening radius (A, 0 = none).  Replaces ElecLJ::set_lambda's per-site
+   interpolation output (src/eleclj.cpp:279-308). */
+int mmnb_set_params(mmnb_handle *h, const int *site_mask, const double *q,
+                    const double *sig, const double *eps, const double *rscreen);
+
+/* One evaluation from HOST arrays.
+   r: 3*nsite site positions.  f: 3*nsite, forces ADDED (may be NULL).
+   u: energy ADDED (may be NULL).  e, phi (nsite), evec (3*nsite): optional
+   outputs of this evaluation (NULL to skip). */
+int mmnb_compute(mmnb_handle *h, const double *r, double *f, double *u,
+                 mmnb_energy *e, double *phi, double *evec);
+
+/* One evaluation on DEVICE arrays, asynchronous on the handle's stream:
+   d_r (3*nsite) positions, d_f (3*nsite) forces ADDED, d_energy (4 doubles,
+   mmnb_energy layout) overwritten.  Any of d_f / d_energy may be NULL.
+   Launches only; no host synchronisation, so it can be captured in a CUDA graph
+   once the handle has done one mmnb_compute (first-call set-up). */
+int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *d_energy);
+
+/* Volume move by factor s: box, eta /= s, Chebyshev table, influence function
+   and cell stencil follow (src/eleclj.cpp:1268-1280, src/pppm.c:643-664). */
+int mmnb_scale(mmnb_handle *h, double s);
+
+/* Bind the handle to a CUDA stream (cudaStream_t passed as void*). */
+int mmnb_set_stream(mmnb_handle *h, void *stream);
+
+/* Neighbour list of the last rebuild, for parity checks against
+   NeighborList (src/nbrlist.cpp:222-251):
+   the unordered group pairs {i, j} of the reference's PairBinary, each once,
+   written as (i, j) with i < j.  *npairs receives the count; pairs (2*cap ints)
+   may be NULL to query the count. */
+int mmnb_get_pairlist(mmnb_handle *h, long *npairs, int *pairs, long cap);
+
+/* Cell of each group at the last rebuild, in the reference's numbering
+   (ix*n + iy)*n + iz (src/nbrlist.cpp:79-82, 228-234). */
+int mmnb_get_cells(mmnb_handle *h, int *cell_of_group, int *ncell_per_dim);
+
+/* Number of list rebuilds so far and number of evaluations. */
+int mmnb_get_counters(mmnb_handle *h, long *rebuilds, long *evaluations);
+
+/* Derived settings: rc, neighbour-list width, eta, P3M mesh (0 if unused). */
+int mmnb_get_settings(mmnb_handle *h, double *rc, double *nlw, double *eta, int mesh[3]);
+
+/* Per-kernel device time (ms) of the last mmnb_compute, when timing is on.
+   Names are written as a comma-separated list into names (size cap). */
+int mmnb_set_timing(mmnb_handle *h, int on);
+int mmnb_get_timing(mmnb_handle *h, double *ms, int nmax, char *names, int cap);
+
+int mmnb_destroy(mmnb_handle *h);
+
+const char *mmnb_last_error(const mmnb_handle *h);
+const char *mmnb_status_string(int status);
+
+/* The erfc(eta r)/r table the FP64 pair kernel reads: 512 segments over r^2,
+   built with the reference's formula (src/rspace.c:25-37, src/cheby.c:7-45).
+   coeff receives 512*7 doubles. */
+int mmnb_chebyshev_table(double rc, double eta, double *min, double *max,
+                         double *inv_dx, double *coeff);
+
+/* Mesh size P3M chooses along a lattice vector of length a (src/pppm.c:277-292,
+   429-431). */
+int mmnb_p3m_mesh_size(double a, double grid_spacing);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MMNB_H */

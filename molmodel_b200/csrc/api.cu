@@ -1,0 +1,1014 @@
+// libmmnb C ABI: handle life cycle, host-side set-up that mirrors ElecLJ::init
+// (src/eleclj.cpp:140-265), and the per-evaluation launch sequence that
+// mirrors ElecLJ::add_to_energy_and_forces (src/eleclj.cpp:785-807).
+
+#include "mmnb_internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <set>
+#include <string>
+#include <tuple>
+#include <vector>
+
+using namespace mmnb;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int fail(mmnb_handle *h, int code, const std::string &msg)
+{
+  if (h)
+    h->err = msg;
+  else
+    g_create_error = msg;
+  return code;
+}
+
+#define CK(call)                                                                                   \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      return fail(h, MMNB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));           \
+  } while (0)
+
+#define CKFFT(call)                                                                                \
+  do {                                                                                             \
+    cufftResult r_ = (call);                                                                       \
+    if (r_ != CUFFT_SUCCESS)                                                                       \
+      return fail(h, MMNB_ERR_CUDA, std::string(#call) + ": cufft error " + std::to_string(r_));   \
+  } while (0)
+
+double sq(double x) { return x * x; }
+
+// 64 machine epsilons, the reference's is_almost_zero (src/fns.c:8-31)
+bool almost_zero(double x) { return fabs(x) < 64 * 2.220446049250313e-16; }
+
+// The reference's Chebyshev table, same formula and operation order
+// (src/cheby.c:7-45, src/rspace.c:18-37); built on the host so it is bitwise
+// the table RSpaceChebyshev_new builds.
+void chebyshev_table(double rhi, double eta, double *mn, double *mx, double *inv_dx, double *coeff7)
+{
+  const double r2max = 1.2 * sq(rhi);
+  const double r2min = r2max > 4 ? 4 : 0.9 * r2max;
+  const double dx = (r2max - r2min) / kCheb;
+  *mn = r2min;
+  *mx = r2max;
+  *inv_dx = 1.0 / dx;
+  for (int i = 0; i < kCheb; i++) {
+    const double a = i * dx + r2min, b = (i + 1) * dx + r2min;
+    double g[50], c[4];
+    const double fac = 2.0 / 50;
+    const double bma = 0.5 * (b - a), bpa = 0.5 * (b + a);
+    for (int k = 0; k < 50; k++) {
+      const double r2 = cos(M_PI * (k + 0.5) / 50) * bma + bpa;
+      const double r = sqrt(r2);
+      g[k] = erfc(eta * r) / r;
+    }
+    for (int j = 0; j < 4; j++) {
+      double s = 0;
+      for (int k = 0; k < 50; k++)
+        s += g[k] * cos(M_PI * j * (k + 0.5) / 50);
+      c[j] = fac * s;
+    }
+    double *o = coeff7 + 7 * i;
+    o[0] = c[0] / 2 - c[1] + c[2] - c[3];
+    o[1] = 2 * c[1] - 8 * c[2] + 18 * c[3];
+    o[2] = 8 * c[2] - 48 * c[3];
+    o[3] = 32 * c[3];
+    o[4] = -2 * o[1] / (b - a);
+    o[5] = -2 * 2 * o[2] / (b - a);
+    o[6] = -2 * 3 * o[3] / (b - a);
+  }
+}
+
+// nearest 2^a 3^b 5^c 7^d; ties keep the first found (src/pppm.c:277-292)
+int near_2357(double x)
+{
+  int best = 1;
+  double bestdiff = fabs(x - 1);
+  for (int p2 = 1; p2 <= x; p2 *= 2)
+    for (int p3 = p2; p3 <= x; p3 *= 3)
+      for (int p5 = p3; p5 <= x; p5 *= 5)
+        for (int p7 = p5; p7 <= x; p7 *= 7) {
+          const double diff = fabs(x - p7);
+          if (diff < bestdiff) {
+            bestdiff = diff;
+            best = p7;
+          }
+        }
+  return best;
+}
+
+unsigned spread_bits(unsigned v)
+{
+  v &= 0x3ff;
+  v = (v | (v << 16)) & 0x030000ff;
+  v = (v | (v << 8)) & 0x0300f00f;
+  v = (v | (v << 4)) & 0x030c30c3;
+  v = (v | (v << 2)) & 0x09249249;
+  return v;
+}
+
+template <typename T>
+int dalloc(mmnb_handle *h, T **p, size_t n)
+{
+  if (*p) {
+    cudaFree(*p);
+    *p = nullptr;
+  }
+  cudaError_t e = cudaMalloc((void **) p, sizeof(T) * (n > 0 ? n : 1));
+  if (e != cudaSuccess)
+    return fail(h, MMNB_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  return MMNB_OK;
+}
+
+template <typename T>
+int upload(mmnb_handle *h, T **p, const std::vector<T> &v)
+{
+  int s = dalloc(h, p, v.size());
+  if (s)
+    return s;
+  if (!v.empty())
+    CK(cudaMemcpy(*p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  return MMNB_OK;
+}
+
+// per-row sorted unique CSR from a pair list, both directions
+void build_csr(int n, const std::vector<std::pair<int, int>> &pairs, std::vector<int> &ptr, std::vector<int> &idx)
+{
+  std::vector<std::vector<int>> rows(n);
+  for (auto &p : pairs) {
+    if (p.first == p.second)
+      continue;
+    rows[p.first].push_back(p.second);
+    rows[p.second].push_back(p.first);
+  }
+  ptr.assign(n + 1, 0);
+  idx.clear();
+  for (int i = 0; i < n; i++) {
+    auto &r = rows[i];
+    std::sort(r.begin(), r.end());
+    r.erase(std::unique(r.begin(), r.end()), r.end());
+    ptr[i + 1] = ptr[i] + (int) r.size();
+    idx.insert(idx.end(), r.begin(), r.end());
+  }
+}
+
+// Cell geometry and stencil (src/nbrlist.cpp:9-17, 84-123).  The reference
+// pairs cell ia with ib = ia + j (mod n) for every half-space offset j with
+// |j_k| <= nmax; as unordered pairs that is the set of wrapped offsets +-j.
+// Offsets whose cells cannot hold two anchors closer than cutoff + width are
+// dropped (anchors sit within half a cell of their cell's lattice point, so
+// along each axis they are at least (|d| - 1) cells apart); the pairs such
+// cells would contribute all fail the distance test, so the list is unchanged.
+int setup_cells(mmnb_handle *h)
+{
+  const int n = (int) floor(cbrt(h->ngroup / 2 + 3));
+  CellGeom &cg = h->cg;
+  cg.n = n;
+  for (int d = 0; d < 3; d++)
+    cg.lc[d] = h->box.L[d] * (1.0 / n);
+  const double cut = h->rc + h->nlw;
+  cg.c2 = sq(cut);
+  h->ncell3 = n * n * n;
+  // reference half stencil
+  double maxdiam;
+  if (h->cfg.bctype == MMNB_CUBIC)
+    maxdiam = sqrt(3.0) * cg.lc[0];
+  else
+    maxdiam = sqrt(cg.lc[0] * cg.lc[0] + cg.lc[1] * cg.lc[1] + cg.lc[2] * cg.lc[2]);
+  const double vol = fabs(cg.lc[0] * cg.lc[1] * cg.lc[2]);
+  const double a01 = sqrt(sq(cg.lc[0] * cg.lc[1])), a02 = sqrt(sq(cg.lc[0] * cg.lc[2])),
+               a12 = sqrt(sq(cg.lc[1] * cg.lc[2]));
+  const double mindiam = vol / std::max(std::max(a01, a02), a12);
+  const double c2cell = sq(cut + maxdiam);
+  const int nmax = std::min((int) ceil((cut + maxdiam) / mindiam), n / 2 + 1);
+  std::set<std::tuple<int, int, int>> full;
+  for (int jx = 0; jx <= nmax; jx++)
+    for (int jy = (jx == 0 ? 0 : -nmax); jy <= nmax; jy++)
+      for (int jz = (jx == 0 && jy == 0 ? 1 : -nmax); jz <= nmax; jz++) {
+        double v[3] = {cg.lc[0] * jx, cg.lc[1] * jy, cg.lc[2] * jz};
+        for (int d = 0; d < 3; d++)
+          v[d] -= cg.lc[d] * floor(v[d] * (1 / cg.lc[d]) + 0.5);
+        if (!(v[0] * v[0] + v[1] * v[1] + v[2] * v[2] < c2cell))
+          continue;
+        for (int sgn = -1; sgn <= 1; sgn += 2) {
+          const int dx = ((sgn * jx) % n + n) % n, dy = ((sgn * jy) % n + n) % n, dz = ((sgn * jz) % n + n) % n;
+          if (dx || dy || dz)
+            full.insert(std::make_tuple(dx, dy, dz));
+        }
+      }
+  const double margin = 1e-6 * std::min(std::min(h->box.L[0], h->box.L[1]), h->box.L[2]) + 1e-12;
+  std::vector<std::pair<double, std::tuple<int, int, int>>> kept;
+  for (auto &t : full) {
+    const int dd[3] = {std::get<0>(t), std::get<1>(t), std::get<2>(t)};
+    double lb2 = 0;
+    for (int d = 0; d < 3; d++) {
+      const int m = std::min(dd[d], n - dd[d]);
+      const double gap = std::max(m - 1, 0) * cg.lc[d];
+      lb2 += gap * gap;
+    }
+    if (sqrt(lb2) <= cut + margin)
+      kept.push_back(std::make_pair(lb2, t));
+  }
+  std::stable_sort(kept.begin(), kept.end(),
+                   [](const std::pair<double, std::tuple<int, int, int>> &a,
+                      const std::pair<double, std::tuple<int, int, int>> &b) { return a.first < b.first; });
+  std::vector<int> st;
+  st.push_back(0);
+  st.push_back(0);
+  st.push_back(0);
+  for (auto &k : kept) {
+    st.push_back(std::get<0>(k.second));
+    st.push_back(std::get<1>(k.second));
+    st.push_back(std::get<2>(k.second));
+  }
+  h->nstencil = (int) st.size() / 3;
+  int s;
+  if ((s = upload(h, &h->d_stencil, st)))
+    return s;
+  // Morton order of cells
+  std::vector<std::pair<unsigned, int>> codes(h->ncell3);
+  for (int ix = 0; ix < n; ix++)
+    for (int iy = 0; iy < n; iy++)
+      for (int iz = 0; iz < n; iz++) {
+        const int c = (ix * n + iy) * n + iz;
+        codes[c] = std::make_pair(spread_bits(ix) | (spread_bits(iy) << 1) | (spread_bits(iz) << 2), c);
+      }
+  std::sort(codes.begin(), codes.end());
+  std::vector<int> rank(h->ncell3), of_rank(h->ncell3);
+  for (int r = 0; r < h->ncell3; r++) {
+    of_rank[r] = codes[r].second;
+    rank[codes[r].second] = r;
+  }
+  if ((s = upload(h, &h->d_cell_rank, rank)) || (s = upload(h, &h->d_cell_of_rank, of_rank)))
+    return s;
+  if ((s = dalloc(h, &h->d_cell_count, h->ncell3)) || (s = dalloc(h, &h->d_cell_start, h->ncell3 + 1)))
+    return s;
+  h->first = true;
+  return MMNB_OK;
+}
+
+int alloc_rows(mmnb_handle *h, int cap)
+{
+  h->rowcap = std::max(1, std::min(cap, h->ngroup));
+  return dalloc(h, &h->d_nbr, (size_t) h->ngroup * h->rowcap);
+}
+
+int initial_rowcap(const mmnb_handle *h)
+{
+  const double rho = h->ngroup / h->volume;
+  const double expect = 4.0 / 3.0 * M_PI * pow(h->rc + h->nlw, 3) * rho + (double) h->ngroup / h->ncell3;
+  const int cap = (int) (1.5 * expect) + 48;
+  return (cap + 31) / 32 * 32;
+}
+
+int setup_cheb(mmnb_handle *h)
+{
+  std::vector<double> c7(kCheb * 7), c8(kCheb * 8, 0.0);
+  chebyshev_table(h->rc, h->eta, &h->cheb_min, &h->cheb_max, &h->cheb_inv_dx, c7.data());
+  for (int i = 0; i < kCheb; i++)
+    for (int k = 0; k < 7; k++)
+      c8[8 * i + k] = c7[7 * i + k];
+  return upload(h, &h->d_cheb, c8);
+}
+
+// reciprocal lattice 2 pi inv(latv)^T of the diagonal box
+void recip_diag(const mmnb_handle *h, double rec[3])
+{
+  for (int d = 0; d < 3; d++)
+    rec[d] = 2 * M_PI * (1.0 / h->box.L[d]);
+}
+
+// ordinary Ewald wave vectors (src/kspace.c:35-71, 96-103)
+int setup_kspace(mmnb_handle *h)
+{
+  const double kc = h->cfg.kspace_cutoff;
+  const double n2max = kc * kc + 1e-8;
+  const int nmax = (int) floor(kc);
+  struct KI { int x, y, z, n2; };
+  std::vector<KI> ks;
+  for (int nx = 0; nx <= nmax; nx++)
+    for (int ny = (nx == 0 ? 0 : -nmax); ny <= nmax; ny++)
+      for (int nz = (nx == 0 && ny == 0 ? 1 : -nmax); nz <= nmax; nz++)
+        if (nx * nx + ny * ny + nz * nz <= n2max)
+          ks.push_back(KI{nx, ny, nz, nx * nx + ny * ny + nz * nz});
+  std::stable_sort(ks.begin(), ks.end(), [](const KI &a, const KI &b) { return a.n2 > b.n2; });
+  h->nk = (int) ks.size();
+  h->kmax = nmax;
+  double rec[3];
+  recip_diag(h, rec);
+  std::vector<double> kv(3 * ks.size()), ak(ks.size());
+  const double c = 0.25 / (h->eta * h->eta), f = 4 * M_PI / h->volume;
+  for (size_t k = 0; k < ks.size(); k++) {
+    kv[3 * k] = rec[0] * ks[k].x;
+    kv[3 * k + 1] = rec[1] * ks[k].y;
+    kv[3 * k + 2] = rec[2] * ks[k].z;
+    const double k2 = kv[3 * k] * kv[3 * k] + kv[3 * k + 1] * kv[3 * k + 1] + kv[3 * k + 2] * kv[3 * k + 2];
+    ak[k] = f * exp(-k2 * c) / k2;
+  }
+  int s;
+  if ((s = upload(h, &h->d_kvecs, kv)) || (s = upload(h, &h->d_ak, ak)) ||
+      (s = dalloc(h, &h->d_skc, 2 * ks.size())))
+    return s;
+  return MMNB_OK;
+}
+
+int setup_p3m(mmnb_handle *h)
+{
+  const mmnb_config &c = h->cfg;
+  if (c.p3m_assignment_order < 2 || c.p3m_assignment_order > kMaxOrder)
+    return fail(h, MMNB_ERR_ARG, "p3m_assignment_order must be 2..7");
+  if (c.p3m_alias_sum_limit < 1 || c.p3m_alias_sum_limit > 8)
+    return fail(h, MMNB_ERR_ARG, "p3m_alias_sum_limit must be 1..8");
+  if (!(c.p3m_grid_spacing > 0))
+    return fail(h, MMNB_ERR_ARG, "p3m_grid_spacing must be > 0");
+  for (int d = 0; d < 3; d++)
+    h->mesh[d] = near_2357(floor(sqrt(sq(h->box.L[d])) / c.p3m_grid_spacing + 0.5));
+  const size_t nr = (size_t) h->mesh[0] * h->mesh[1] * h->mesh[2];
+  const size_t nk = (size_t) h->mesh[0] * h->mesh[1] * (h->mesh[2] / 2 + 1);
+  int s;
+  if ((s = dalloc(h, &h->d_green, nk)) || (s = dalloc(h, &h->d_kvec, 3 * nk)))
+    return s;
+  if (c.precision == MMNB_FP64 || c.p3m_ik_differentiate) {
+    if ((s = dalloc(h, &h->d_mesh, nr * (c.p3m_ik_differentiate ? 1 : 1))) || (s = dalloc(h, &h->d_meshk, nk)))
+      return s;
+    CKFFT(cufftPlan3d(&h->plan_r2c, h->mesh[0], h->mesh[1], h->mesh[2], CUFFT_D2Z));
+    CKFFT(cufftPlan3d(&h->plan_c2r, h->mesh[0], h->mesh[1], h->mesh[2], CUFFT_Z2D));
+    CKFFT(cufftSetStream(h->plan_r2c, h->stream));
+    CKFFT(cufftSetStream(h->plan_c2r, h->stream));
+    if (c.p3m_ik_differentiate)
+      if ((s = dalloc(h, &h->d_egrid, 3 * nr)) || (s = dalloc(h, &h->d_egridk, 3 * nk)))
+        return s;
+  }
+  CK(launch_p3m_green(h));
+  double chi = 0;
+  CK(cudaMemcpyAsync(&chi, h->d_energy, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->p3m_chi = pow(1.0 / h->volume, 1.0 / 3.0) * sqrt(2 * fabs(chi));
+  h->p3m = true;
+  return MMNB_OK;
+}
+
+void free_all(mmnb_handle *h)
+{
+  void *ptrs[] = {h->d_group, h->d_excl_ptr, h->d_excl_idx, h->d_p14_ptr, h->d_p14_idx, h->d_gexcl_ptr,
+                  h->d_gexcl_idx, h->d_mask, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_cheb,
+                  h->d_stencil, h->d_cell_rank, h->d_cell_of_rank, h->d_cell_of_group, h->d_cell_count,
+                  h->d_cell_start, h->d_slot, h->d_sorted, h->d_rank, h->d_anchor, h->d_last, h->d_anchor_sorted,
+                  h->d_top2, h->d_nbr, h->d_nbr_count, h->d_flags, h->d_sr, h->d_sp, h->d_site_of_slot,
+                  h->d_phi, h->d_evec, h->d_ljf, h->d_lj_part, h->d_elec_part, h->d_energy, h->d_r, h->d_f,
+                  h->d_mesh, h->d_meshk, h->d_green, h->d_kvec, h->d_egrid, h->d_egridk, h->d_mesh32,
+                  h->d_meshk32, h->d_green32, h->d_mesh_fx, h->d_kint, h->d_kvecs, h->d_ak, h->d_skc,
+                  h->mx.site_xyzq, h->mx.site_lj, h->mx.site_mask, h->mx.anchor, h->mx.acc};
+  for (void *p : ptrs)
+    if (p)
+      cudaFree(p);
+  if (h->h_flags)
+    cudaFreeHost(h->h_flags);
+  if (h->h_f)
+    cudaFreeHost(h->h_f);
+  if (h->h_out)
+    cudaFreeHost(h->h_out);
+  if (h->plan_r2c)
+    cufftDestroy(h->plan_r2c);
+  if (h->plan_c2r)
+    cufftDestroy(h->plan_c2r);
+  if (h->plan_r2c32)
+    cufftDestroy(h->plan_r2c32);
+  if (h->plan_c2r32)
+    cufftDestroy(h->plan_c2r32);
+  for (auto e : h->timing.ev)
+    cudaEventDestroy(e);
+}
+
+}  // namespace
+
+namespace mmnb {
+
+void timing_mark(mmnb_handle *h, const char *name)
+{
+  if (!h->timing.on)
+    return;
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  cudaEventRecord(e, h->stream);
+  h->timing.ev.push_back(e);
+  h->timing.names.push_back(name);
+}
+
+}  // namespace mmnb
+
+extern "C" {
+
+int mmnb_config_init(mmnb_config *c)
+{
+  if (!c)
+    return MMNB_ERR_ARG;
+  memset(c, 0, sizeof(*c));
+  c->precision = MMNB_FP64;
+  c->bctype = MMNB_CUBIC;
+  c->rspace_cutoff = 0;
+  c->smoothing_width = 1;
+  c->neighbor_list_width = 0;
+  c->kspace_cutoff = 5;
+  c->ewald_screening = -1;
+  c->use_p3m = 0;
+  c->p3m_grid_spacing = 0.5;
+  c->p3m_assignment_order = 3;
+  c->p3m_alias_sum_limit = 2;
+  c->p3m_ik_differentiate = 0;
+  c->include_lj_correction = 1;
+  c->geometric_combining_for_sigma = 0;
+  c->include_rspace = 1;
+  c->include_kspace = 1;
+  c->include_self = 1;
+  c->elec_1_4_scale_factor = 1;
+  c->lj_1_4_scale_factor = 1;
+  c->rebuild_interval = 0;
+  c->device = -1;
+  return MMNB_OK;
+}
+
+static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngroup, const int *group, int nexcl,
+                       const int *excl, int n14, const int *pairs14)
+{
+  h->cfg = *c;
+  if (c->precision != MMNB_FP64 && c->precision != MMNB_MIXED)
+    return fail(h, MMNB_ERR_ARG, "precision must be MMNB_FP64 or MMNB_MIXED");
+  if (c->bctype != MMNB_CUBIC && c->bctype != MMNB_ORTHORHOMBIC)
+    return fail(h, MMNB_ERR_UNSUPPORTED, "only cubic and orthorhombic boundary conditions are supported");
+  if (nsite <= 0 || ngroup <= 0 || !group)
+    return fail(h, MMNB_ERR_ARG, "nsite and ngroup must be positive and group non-null");
+  if ((nexcl > 0 && !excl) || (n14 > 0 && !pairs14) || nexcl < 0 || n14 < 0)
+    return fail(h, MMNB_ERR_ARG, "exclusion or 1-4 arrays missing");
+  h->nsite = nsite;
+  h->ngroup = ngroup;
+  // box
+  for (int d = 0; d < 3; d++) {
+    const double L = c->bctype == MMNB_CUBIC ? c->box[0] : c->box[d];
+    if (!(L > 0))
+      return fail(h, MMNB_ERR_ARG, "box lengths must be > 0");
+    h->box.L[d] = L;
+    h->box.invL[d] = 1 / L;
+  }
+  h->volume = h->box.L[0] * h->box.L[1] * h->box.L[2];
+  h->min_diameter = std::min(std::min(h->box.L[0], h->box.L[1]), h->box.L[2]);
+  // groups: contiguous, covering every site once
+  h->group.assign(group, group + 2 * (size_t) ngroup);
+  h->group_of_site.assign(nsite, -1);
+  h->maxgs = 1;
+  for (int g = 0; g < ngroup; g++) {
+    const int a = group[2 * g], b = group[2 * g + 1];
+    if (a < 0 || b > nsite || b <= a)
+      return fail(h, MMNB_ERR_ARG, "group " + std::to_string(g) + " has an invalid site range");
+    h->maxgs = std::max(h->maxgs, b - a);
+    for (int s = a; s < b; s++) {
+      if (h->group_of_site[s] >= 0)
+        return fail(h, MMNB_ERR_ARG, "site " + std::to_string(s) + " belongs to two groups");
+      h->group_of_site[s] = g;
+    }
+  }
+  for (int s = 0; s < nsite; s++)
+    if (h->group_of_site[s] < 0)
+      return fail(h, MMNB_ERR_ARG, "site " + std::to_string(s) + " belongs to no group");
+  if (h->maxgs > kMaxGroup)
+    return fail(h, MMNB_ERR_UNSUPPORTED, "groups of more than 8 sites are not supported");
+  h->G = h->maxgs <= 4 ? h->maxgs : 8;
+  // cutoff, skin (src/eleclj.cpp:164-182)
+  h->rc = c->rspace_cutoff;
+  if (almost_zero(h->rc))
+    h->rc = 0.45 * h->min_diameter;
+  if (h->rc > 0.49 * h->min_diameter || !(h->rc > 0))
+    return fail(h, MMNB_ERR_CUTOFF, "rspace_cutoff must be <= 0.49 * minimum diameter of box");
+  if (c->smoothing_width >= h->rc || c->smoothing_width < 0)
+    return fail(h, MMNB_ERR_CUTOFF, "smoothing_width must be less than the real-space cutoff");
+  h->nlw = c->neighbor_list_width;
+  if (almost_zero(h->nlw)) {
+    h->nlw = 0.2 * h->rc;
+    if (h->rc + h->nlw >= 0.5 * h->min_diameter)
+      h->nlw = 0.499 * h->min_diameter - h->rc;
+  }
+  if (h->nlw < 0)
+    return fail(h, MMNB_ERR_ARG, "neighbor_list_width must be >= 0");
+  h->rhi2 = sq(h->rc);
+  h->rlo2 = sq(h->rc - c->smoothing_width);
+  // Ewald parameter (src/eleclj.cpp:189-239)
+  h->eta = c->ewald_screening;
+  if (c->include_kspace && c->use_p3m) {
+    if (!(h->eta > 0))
+      return fail(h, MMNB_ERR_UNSUPPORTED,
+                  "P3M needs an explicit ewald_screening > 0 (eta optimisation is not provided)");
+  } else if (h->eta < 0) {
+    h->eta = sqrt((M_PI * c->kspace_cutoff) / (h->rc * h->min_diameter));
+  }
+  if (!(h->eta > 0))
+    return fail(h, MMNB_ERR_ARG, "ewald_screening must be > 0");
+  // topology tables
+  std::vector<std::pair<int, int>> ep, pp;
+  for (int k = 0; k < nexcl; k++) {
+    const int i = excl[2 * k], j = excl[2 * k + 1];
+    if (i < 0 || j < 0 || i >= nsite || j >= nsite)
+      return fail(h, MMNB_ERR_ARG, "exclusion pair out of range");
+    ep.push_back(std::make_pair(i, j));
+  }
+  build_csr(nsite, ep, h->excl_ptr, h->excl_idx);
+  h->use_14 = !almost_zero(c->elec_1_4_scale_factor - 1) || !almost_zero(c->lj_1_4_scale_factor - 1);
+  if (h->use_14)
+    for (int k = 0; k < n14; k++) {
+      const int i = pairs14[2 * k], j = pairs14[2 * k + 1];
+      if (i < 0 || j < 0 || i >= nsite || j >= nsite)
+        return fail(h, MMNB_ERR_ARG, "1-4 pair out of range");
+      pp.push_back(std::make_pair(i, j));
+    }
+  build_csr(nsite, pp, h->p14_ptr, h->p14_idx);
+  std::vector<std::pair<int, int>> gp;
+  for (auto &e : ep) {
+    const int gi = h->group_of_site[e.first], gj = h->group_of_site[e.second];
+    if (gi != gj)
+      gp.push_back(std::make_pair(gi, gj));
+  }
+  build_csr(ngroup, gp, h->gexcl_ptr, h->gexcl_idx);
+  h->any_gexcl = !h->gexcl_idx.empty();
+  // device
+  if (c->device >= 0)
+    CK(cudaSetDevice(c->device));
+  CK(cudaGetDevice(&h->dev));
+  CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  int s;
+  std::vector<int> gvec(h->group);
+  if ((s = upload(h, &h->d_group, gvec)) || (s = upload(h, &h->d_excl_ptr, h->excl_ptr)) ||
+      (s = upload(h, &h->d_excl_idx, h->excl_idx)) || (s = upload(h, &h->d_p14_ptr, h->p14_ptr)) ||
+      (s = upload(h, &h->d_p14_idx, h->p14_idx)) || (s = upload(h, &h->d_gexcl_ptr, h->gexcl_ptr)) ||
+      (s = upload(h, &h->d_gexcl_idx, h->gexcl_idx)))
+    return s;
+  if ((s = dalloc(h, &h->d_mask, nsite)) || (s = dalloc(h, &h->d_q, nsite)) || (s = dalloc(h, &h->d_sig, nsite)) ||
+      (s = dalloc(h, &h->d_eps, nsite)) || (s = dalloc(h, &h->d_rscreen, nsite)))
+    return s;
+  if ((s = dalloc(h, &h->d_cell_of_group, ngroup)) || (s = dalloc(h, &h->d_slot, ngroup)) ||
+      (s = dalloc(h, &h->d_sorted, ngroup)) || (s = dalloc(h, &h->d_rank, ngroup)) ||
+      (s = dalloc(h, &h->d_anchor, 3 * (size_t) ngroup)) || (s = dalloc(h, &h->d_last, 3 * (size_t) ngroup)) ||
+      (s = dalloc(h, &h->d_anchor_sorted, 3 * (size_t) ngroup)) || (s = dalloc(h, &h->d_nbr_count, ngroup)) ||
+      (s = dalloc(h, &h->d_flags, kFlagCount)))
+    return s;
+  CK(cudaMemset(h->d_last, 0, sizeof(double) * 3 * ngroup));
+  CK(cudaMemset(h->d_flags, 0, sizeof(int) * kFlagCount));
+  CK(cudaMallocHost((void **) &h->h_flags, sizeof(int) * kFlagCount));
+  h->top2_blocks = std::min(256, div_up(ngroup, 256));
+  if ((s = dalloc(h, &h->d_top2, 2 * (size_t) h->top2_blocks)))
+    return s;
+  const size_t nslot = (size_t) ngroup * h->G;
+  if ((s = dalloc(h, &h->d_sr, nslot)) || (s = dalloc(h, &h->d_sp, nslot)) ||
+      (s = dalloc(h, &h->d_site_of_slot, nslot)))
+    return s;
+  h->elec_blocks = div_up(nsite, 256);
+  if ((s = dalloc(h, &h->d_phi, nsite)) || (s = dalloc(h, &h->d_evec, 3 * (size_t) nsite)) ||
+      (s = dalloc(h, &h->d_ljf, 3 * (size_t) nsite)) || (s = dalloc(h, &h->d_lj_part, (size_t) ngroup + nsite)) ||
+      (s = dalloc(h, &h->d_elec_part, h->elec_blocks)) || (s = dalloc(h, &h->d_energy, 8)) ||
+      (s = dalloc(h, &h->d_r, 3 * (size_t) nsite)) || (s = dalloc(h, &h->d_f, 3 * (size_t) nsite)))
+    return s;
+  CK(cudaMemset(h->d_lj_part, 0, sizeof(double) * ((size_t) ngroup + nsite)));
+  CK(cudaMallocHost((void **) &h->h_f, sizeof(double) * 3 * (size_t) nsite));
+  CK(cudaMallocHost((void **) &h->h_out, sizeof(double) * 16));
+  if ((s = setup_cells(h)))
+    return s;
+  if ((s = alloc_rows(h, initial_rowcap(h))))
+    return s;
+  if ((s = setup_cheb(h)))
+    return s;
+  if (c->include_kspace) {
+    if (c->use_p3m) {
+      if ((s = setup_p3m(h)))
+        return s;
+    } else {
+      h->kspace = true;
+      if ((s = setup_kspace(h)))
+        return s;
+    }
+  }
+  return MMNB_OK;
+}
+
+int mmnb_create(const mmnb_config *c, int nsite, int ngroup, const int *group, int nexcl, const int *excl, int n14,
+                const int *pairs14, mmnb_handle **out)
+{
+  if (!c || !out)
+    return fail(nullptr, MMNB_ERR_ARG, "null config or output pointer");
+  *out = nullptr;
+  mmnb_handle *h = new mmnb_handle;
+  const int s = create_impl(h, c, nsite, ngroup, group, nexcl, excl, n14, pairs14);
+  if (s) {
+    g_create_error = h->err;
+    free_all(h);
+    if (h->stream)
+      cudaStreamDestroy(h->stream);
+    delete h;
+    return s;
+  }
+  *out = h;
+  return MMNB_OK;
+}
+
+// The reference's LJ tail (src/eleclj.cpp:1247-1266).
+static double lj_tail(const mmnb_handle *h)
+{
+  const double rhi = h->rc, rlo = rhi - h->cfg.smoothing_width;
+  const double A = h->totA, B = h->totB;
+  const double rlo2 = rlo * rlo, rlo3 = rlo2 * rlo, rlo4 = rlo3 * rlo;
+  const double rlo5 = rlo4 * rlo, rlo6 = rlo5 * rlo, rlo7 = rlo6 * rlo, rlo9 = rlo7 * rlo2;
+  const double rhi2 = rhi * rhi, rhi3 = rhi2 * rhi, rhi4 = rhi3 * rhi, rhi5 = rhi4 * rhi;
+  const double rhi6 = rhi5 * rhi, rhi7 = rhi6 * rhi;
+  return 2 * M_PI / h->volume *
+         (A / (9 * rlo9) + B / (3 * rlo3) -
+          (rhi - rlo) / (63 * rhi3 * rlo9 * pow(rhi + rlo, 5)) *
+              (3 * B * rhi3 * rlo6 * (7 * rhi4 + 42 * rhi3 * rlo + 112 * rhi2 * rlo2 + 150 * rhi * rlo3 + 25 * rlo4) +
+               A * (7 * rhi7 + 42 * rhi6 * rlo + 112 * rhi5 * rlo2 + 182 * rhi4 * rlo3 + 217 * rhi3 * rlo4 +
+                    224 * rhi2 * rlo5 + 192 * rhi * rlo6 + 32 * rlo7)));
+}
+
+static void update_energy_constants(mmnb_handle *h, double qsum)
+{
+  h->lj_correction = lj_tail(h);
+  h->neutral_b = almost_zero(qsum) ? 0 : -M_PI / (sq(h->eta) * h->volume) * qsum;
+}
+
+int mmnb_set_params(mmnb_handle *h, const int *site_mask, const double *q, const double *sig, const double *eps,
+                    const double *rscreen)
+{
+  if (!h || !site_mask || !q || !sig || !eps)
+    return fail(h, MMNB_ERR_ARG, "null parameter array");
+  const int n = h->nsite;
+  std::vector<double> rs(n, 0.0);
+  h->any_q = h->any_lj = h->has_rscreen = false;
+  double qsum = 0;
+  for (int i = 0; i < n; i++) {
+    if (site_mask[i] & MMNB_SITE_HAS_Q)
+      h->any_q = true;
+    if (site_mask[i] & MMNB_SITE_HAS_LJ) {
+      h->any_lj = true;
+      if (!(sig[i] > 0) || eps[i] < 0)
+        return fail(h, MMNB_ERR_ARG, "LJ sites need sigma > 0 and epsilon >= 0");
+    }
+    if (rscreen) {
+      if (rscreen[i] < 0)
+        return fail(h, MMNB_ERR_ARG, "screening radius must be >= 0");
+      rs[i] = rscreen[i];
+      if (rscreen[i] > 0)
+        h->has_rscreen = true;
+    }
+    qsum += q[i];
+  }
+  CK(cudaMemcpy(h->d_mask, site_mask, sizeof(int) * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_q, q, sizeof(double) * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_sig, sig, sizeof(double) * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_eps, eps, sizeof(double) * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_rscreen, rs.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+  // LJ tail totals over distinct (sigma, epsilon) printed as %12.6g
+  // (src/eleclj.cpp:283-308)
+  struct T { double s, e; long n; };
+  std::vector<T> ty;
+  for (int i = 0; i < n; i++) {
+    if (!(site_mask[i] & MMNB_SITE_HAS_LJ))
+      continue;
+    char key[128];
+    double sv, ev;
+    snprintf(key, sizeof key, "%12.6g %12.6g", sig[i], eps[i]);
+    sscanf(key, "%lf%lf", &sv, &ev);
+    size_t a = 0;
+    for (; a < ty.size(); a++)
+      if (ty[a].s == sv && ty[a].e == ev)
+        break;
+    if (a == ty.size())
+      ty.push_back(T{sv, ev, 0});
+    ty[a].n++;
+  }
+  h->totA = h->totB = 0;
+  for (auto &a : ty)
+    for (auto &b : ty) {
+      const double s6 = pow(h->cfg.geometric_combining_for_sigma ? sqrt(a.s * b.s) : 0.5 * (a.s + b.s), 6);
+      const double bb = 4 * sqrt(a.e * b.e) * a.n * b.n * s6;
+      h->totB -= bb;
+      h->totA += bb * s6;
+    }
+  update_energy_constants(h, qsum);
+  h->params_set = true;
+  return MMNB_OK;
+}
+
+int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *d_energy)
+{
+  if (!h || !d_r)
+    return fail(h, MMNB_ERR_ARG, "null handle or positions");
+  if (!h->params_set)
+    return fail(h, MMNB_ERR_STATE, "mmnb_set_params has not been called");
+  if (h->cfg.precision == MMNB_MIXED)
+    return fail(h, MMNB_ERR_UNSUPPORTED, "mixed precision is not available in this build");
+  double *energy = d_energy ? d_energy : h->d_energy;
+  timing_mark(h, "start");
+  CK(launch_gather_anchors(h, d_r));
+  CK(launch_rebuild_decide(h, h->force_rebuild_next));
+  CK(launch_build_list(h));
+  timing_mark(h, "nbrlist");
+  CK(launch_sort_sites(h, d_r));
+  if (h->cfg.include_rspace) {
+    CK(launch_rspace_fp64(h));
+    timing_mark(h, "rspace_pair");
+    CK(launch_exclusions(h, d_r));
+    timing_mark(h, "rspace_excl");
+  } else {
+    CK(cudaMemsetAsync(h->d_phi, 0, sizeof(double) * h->nsite, h->stream));
+    CK(cudaMemsetAsync(h->d_evec, 0, sizeof(double) * 3 * h->nsite, h->stream));
+    CK(cudaMemsetAsync(h->d_ljf, 0, sizeof(double) * 3 * h->nsite, h->stream));
+    CK(cudaMemsetAsync(h->d_lj_part, 0, sizeof(double) * (h->ngroup + h->nsite), h->stream));
+  }
+  if (h->any_q && h->cfg.include_kspace) {
+    if (h->p3m)
+      CK(launch_p3m_fp64(h, d_r));
+    else if (h->kspace)
+      CK(launch_kspace(h, d_r));
+    timing_mark(h, "kspace");
+  }
+  CK(launch_finalize(h, d_f, energy));
+  timing_mark(h, "finalize");
+  h->first = false;
+  h->force_rebuild_next = 0;
+  h->evals++;
+  return MMNB_OK;
+}
+
+int mmnb_compute(mmnb_handle *h, const double *r, double *f, double *u, mmnb_energy *e, double *phi, double *evec)
+{
+  if (!h || !r)
+    return fail(h, MMNB_ERR_ARG, "null handle or positions");
+  const size_t n3 = 3 * (size_t) h->nsite;
+  for (int attempt = 0; attempt < 2; attempt++) {
+    if (h->timing.on) {
+      for (auto ev : h->timing.ev)
+        cudaEventDestroy(ev);
+      h->timing.ev.clear();
+      h->timing.names.clear();
+    }
+    CK(cudaMemcpyAsync(h->d_r, r, sizeof(double) * n3, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(h->d_f, 0, sizeof(double) * n3, h->stream));
+    CK(cudaMemsetAsync(h->d_flags + kFlagOverflow, 0, sizeof(int), h->stream));
+    const int s = mmnb_compute_device(h, h->d_r, h->d_f, h->d_energy);
+    if (s)
+      return s;
+    CK(cudaMemcpyAsync(h->h_f, h->d_f, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->h_out, h->d_energy, sizeof(double) * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->h_flags, h->d_flags, sizeof(int) * kFlagCount, cudaMemcpyDeviceToHost, h->stream));
+    if (phi)
+      CK(cudaMemcpyAsync(phi, h->d_phi, sizeof(double) * h->nsite, cudaMemcpyDeviceToHost, h->stream));
+    if (evec)
+      CK(cudaMemcpyAsync(evec, h->d_evec, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->rebuilds = h->h_flags[5];
+    if (h->h_flags[kFlagOverflow] > 0) {
+      // a row outgrew its capacity: grow, force a rebuild, evaluate again
+      const int need = h->h_flags[kFlagOverflow];
+      int st = alloc_rows(h, (need + need / 4 + 63) / 32 * 32);
+      if (st)
+        return st;
+      h->force_rebuild_next = 1;
+      h->evals--;
+      continue;
+    }
+    if (f)
+      for (size_t i = 0; i < n3; i++)
+        f[i] += h->h_f[i];
+    if (u)
+      *u += h->h_out[3];
+    if (e) {
+      e->elec = h->h_out[0];
+      e->lj = h->h_out[1];
+      e->lj_correction = h->h_out[2];
+      e->total = h->h_out[3];
+    }
+    if (h->timing.on) {
+      h->timing.ms.clear();
+      for (size_t k = 1; k < h->timing.ev.size(); k++) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, h->timing.ev[k - 1], h->timing.ev[k]);
+        h->timing.ms.push_back(ms);
+      }
+    }
+    return MMNB_OK;
+  }
+  return fail(h, MMNB_ERR_OVERFLOW, "neighbour rows overflowed twice");
+}
+
+__global__ void k_scale_green(long nk, double s, double *green, double *kvec)
+{
+  const long g = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nk)
+    return;
+  green[g] /= s;
+  kvec[3 * g] /= s;
+  kvec[3 * g + 1] /= s;
+  kvec[3 * g + 2] /= s;
+}
+
+int mmnb_scale(mmnb_handle *h, double s)
+{
+  if (!h || !(s > 0))
+    return fail(h, MMNB_ERR_ARG, "scale factor must be > 0");
+  for (int d = 0; d < 3; d++) {
+    h->box.L[d] *= s;
+    h->box.invL[d] = 1 / h->box.L[d];
+  }
+  h->volume = h->box.L[0] * h->box.L[1] * h->box.L[2];
+  h->min_diameter = std::min(std::min(h->box.L[0], h->box.L[1]), h->box.L[2]);
+  h->eta *= 1 / s;
+  int st;
+  if ((st = setup_cheb(h)))
+    return st;
+  if (h->p3m) {
+    const long nk = (long) h->mesh[0] * h->mesh[1] * (h->mesh[2] / 2 + 1);
+    k_scale_green<<<div_up(nk, 256), 256, 0, h->stream>>>(nk, s, h->d_green, h->d_kvec);
+    CK(cudaGetLastError());
+  }
+  if (h->kspace && (st = setup_kspace(h)))
+    return st;
+  if ((st = setup_cells(h)))
+    return st;
+  // q sum for the neutralising term
+  std::vector<double> q(h->nsite);
+  CK(cudaMemcpy(q.data(), h->d_q, sizeof(double) * h->nsite, cudaMemcpyDeviceToHost));
+  double qsum = 0;
+  for (double v : q)
+    qsum += v;
+  update_energy_constants(h, qsum);
+  CK(cudaStreamSynchronize(h->stream));
+  return MMNB_OK;
+}
+
+int mmnb_set_stream(mmnb_handle *h, void *stream)
+{
+  if (!h)
+    return MMNB_ERR_ARG;
+  h->stream = (cudaStream_t) stream;
+  if (h->plan_r2c)
+    CKFFT(cufftSetStream(h->plan_r2c, h->stream));
+  if (h->plan_c2r)
+    CKFFT(cufftSetStream(h->plan_c2r, h->stream));
+  if (h->plan_r2c32)
+    CKFFT(cufftSetStream(h->plan_r2c32, h->stream));
+  if (h->plan_c2r32)
+    CKFFT(cufftSetStream(h->plan_c2r32, h->stream));
+  return MMNB_OK;
+}
+
+int mmnb_get_pairlist(mmnb_handle *h, long *npairs, int *pairs, long cap)
+{
+  if (!h || !npairs)
+    return fail(h, MMNB_ERR_ARG, "null argument");
+  if (h->evals == 0)
+    return fail(h, MMNB_ERR_STATE, "no evaluation yet");
+  std::vector<int> cnt(h->ngroup), sorted(h->ngroup), rows((size_t) h->ngroup * h->rowcap);
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaMemcpy(cnt.data(), h->d_nbr_count, sizeof(int) * h->ngroup, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(sorted.data(), h->d_sorted, sizeof(int) * h->ngroup, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(rows.data(), h->d_nbr, sizeof(int) * rows.size(), cudaMemcpyDeviceToHost));
+  long k = 0;
+  for (int p = 0; p < h->ngroup; p++) {
+    const int gi = sorted[p];
+    for (int e = 0; e < cnt[p]; e++) {
+      const int gj = sorted[rows[(size_t) p * h->rowcap + e]];
+      if (gi < gj) {
+        if (pairs && k < cap) {
+          pairs[2 * k] = gi;
+          pairs[2 * k + 1] = gj;
+        }
+        k++;
+      }
+    }
+  }
+  *npairs = k;
+  return MMNB_OK;
+}
+
+int mmnb_get_cells(mmnb_handle *h, int *cell_of_group, int *ncell_per_dim)
+{
+  if (!h)
+    return MMNB_ERR_ARG;
+  if (ncell_per_dim)
+    *ncell_per_dim = h->cg.n;
+  if (cell_of_group) {
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(cell_of_group, h->d_cell_of_group, sizeof(int) * h->ngroup, cudaMemcpyDeviceToHost));
+  }
+  return MMNB_OK;
+}
+
+int mmnb_get_counters(mmnb_handle *h, long *rebuilds, long *evaluations)
+{
+  if (!h)
+    return MMNB_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  int fl[kFlagCount];
+  CK(cudaMemcpy(fl, h->d_flags, sizeof(fl), cudaMemcpyDeviceToHost));
+  if (rebuilds)
+    *rebuilds = fl[5];
+  if (evaluations)
+    *evaluations = fl[4];
+  return MMNB_OK;
+}
+
+int mmnb_get_settings(mmnb_handle *h, double *rc, double *nlw, double *eta, int mesh[3])
+{
+  if (!h)
+    return MMNB_ERR_ARG;
+  if (rc)
+    *rc = h->rc;
+  if (nlw)
+    *nlw = h->nlw;
+  if (eta)
+    *eta = h->eta;
+  if (mesh)
+    for (int d = 0; d < 3; d++)
+      mesh[d] = h->mesh[d];
+  return MMNB_OK;
+}
+
+int mmnb_set_timing(mmnb_handle *h, int on)
+{
+  if (!h)
+    return MMNB_ERR_ARG;
+  h->timing.on = on != 0;
+  return MMNB_OK;
+}
+
+int mmnb_get_timing(mmnb_handle *h, double *ms, int nmax, char *names, int cap)
+{
+  if (!h)
+    return MMNB_ERR_ARG;
+  const int n = (int) h->timing.ms.size();
+  std::string all;
+  for (int k = 0; k < n; k++) {
+    if (ms && k < nmax)
+      ms[k] = h->timing.ms[k];
+    if (k)
+      all += ",";
+    all += h->timing.names[k + 1];
+  }
+  if (names && cap > 0) {
+    strncpy(names, all.c_str(), cap - 1);
+    names[cap - 1] = 0;
+  }
+  return n;
+}
+
+int mmnb_destroy(mmnb_handle *h)
+{
+  if (!h)
+    return MMNB_OK;
+  if (h->stream)
+    cudaStreamSynchronize(h->stream);
+  free_all(h);
+  if (h->stream)
+    cudaStreamDestroy(h->stream);
+  delete h;
+  return MMNB_OK;
+}
+
+const char *mmnb_last_error(const mmnb_handle *h)
+{
+  return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+const char *mmnb_status_string(int status)
+{
+  switch (status) {
+  case MMNB_OK: return "ok";
+  case MMNB_ERR_ARG: return "bad argument";
+  case MMNB_ERR_CUDA: return "CUDA error";
+  case MMNB_ERR_UNSUPPORTED: return "unsupported option";
+  case MMNB_ERR_CUTOFF: return "cutoff too large for the box";
+  case MMNB_ERR_OVERFLOW: return "neighbour list overflow";
+  case MMNB_ERR_STATE: return "call out of order";
+  case MMNB_ERR_TIMEOUT: return "device wait timed out";
+  case MMNB_ERR_DEVICE: return "device-side check failed";
+  default: return "unknown status";
+  }
+}
+
+int mmnb_chebyshev_table(double rc, double eta, double *min, double *max, double *inv_dx, double *coeff)
+{
+  if (!min || !max || !inv_dx || !coeff || !(rc > 0) || !(eta > 0))
+    return MMNB_ERR_ARG;
+  chebyshev_table(rc, eta, min, max, inv_dx, coeff);
+  return MMNB_OK;
+}
+
+int mmnb_p3m_mesh_size(double a, double grid_spacing)
+{
+  if (!(a > 0) || !(grid_spacing > 0))
+    return 0;
+  return near_2357(floor(a / grid_spacing + 0.5));
+}
+
+}  // extern "C"

@@ -1,0 +1,363 @@
+// P3M reciprocal space on the GPU (replaces p3m_init / p3m_field,
+// src/pppm.c:313-393, 498-641).
+//
+// Steps per evaluation: B-spline charge assignment onto the mesh, cuFFT
+// real-to-complex, multiplication by the optimal influence function,
+// complex-to-real, interpolation of potential and field back to the sites.
+// Differentiation is in real space (gradient of the assignment function,
+// the reference default) or, with p3m_ik_differentiate, by -ik on the mesh
+// with three extra inverse transforms.
+//
+// Charge-assignment weights come from the Cox-de Boor recursion for cardinal
+// B-splines, which reproduces the reference's per-order polynomials
+// (src/pppm.c:69-275) for every order 2..7.  The influence function is the
+// Hockney-Eastwood optimum with an alias sum over |p| <= nalias, evaluated
+// once per box on the GPU in FP64.
+
+#include "mmnb_internal.cuh"
+
+namespace mmnb {
+
+struct MeshArgs {
+  int n[3];
+  double A[9];      // mesh-scaled inverse lattice, tensor_t layout: s = A r
+  int nsite;
+};
+
+// Weights W[p] and negated derivatives ND[p] for mesh points j + lo + p,
+// where s is the particle's mesh coordinate (src/pppm.c:533-557).
+template <int P, typename T>
+__device__ __forceinline__ int bspline_weights(T s, T *W, T *ND)
+{
+  int j;
+  T delta;
+  if (P % 2) {
+    j = (int) floor(s + T(0.5));
+    delta = s - T(j);
+  } else {
+    j = (int) floor(s);
+    delta = s - (T(j) + T(0.5));
+  }
+  const T w = delta + T(0.5);
+  T m[P], prev[P];
+  m[0] = T(1);
+#pragma unroll
+  for (int k = 2; k <= P; k++) {
+    const T inv = T(1) / T(k - 1);
+#pragma unroll
+    for (int i = 0; i < k - 1; i++)
+      prev[i] = m[i];
+#pragma unroll
+    for (int i = 0; i < k; i++) {
+      const T a = i < k - 1 ? prev[i] : T(0);
+      const T b = i > 0 ? prev[i - 1] : T(0);
+      m[i] = ((w + T(i)) * a + (T(k) - w - T(i)) * b) * inv;
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < P; p++) {
+    const int i = P - 1 - p;
+    W[p] = m[i];
+    const T a = i < P - 1 ? prev[i] : T(0);
+    const T b = i > 0 ? prev[i - 1] : T(0);
+    ND[p] = b - a;
+  }
+  return j - ((P + 1) / 2 - 1);
+}
+
+__device__ __forceinline__ int wrap_idx(int i, int n)
+{
+  i %= n;
+  return i < 0 ? i + n : i;
+}
+
+// ---- influence function -----------------------------------------------------
+
+struct GreenArgs {
+  int n[3];
+  int nalias, order, ik;
+  double rec[9];     // 2 pi inv(latv)^T, tensor_t layout
+  double inv_v, inv_4eta2;
+  double *green, *kvec, *chi;
+};
+
+__device__ __forceinline__ double sincpi_d(double x)
+{
+  const double y = M_PI * x;
+  return fabs(y) < 1e-16 ? 1 - y * y / 6 : sin(y) / y;
+}
+
+__global__ void k_green(GreenArgs a)
+{
+  const int nx = a.n[0], ny = a.n[1], nz = a.n[2], nzh = nz / 2 + 1;
+  const long g = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (long) nx * ny * nzh)
+    return;
+  const int iz = (int) (g % nzh);
+  const int iy = (int) ((g / nzh) % ny);
+  const int ix = (int) (g / ((long) nzh * ny));
+  const double jx = ix > nx / 2 ? ix - nx : ix;
+  const double jy = iy > ny / 2 ? iy - ny : iy;
+  const double jz = iz;
+  const double *R = a.rec;
+  double kv[3];
+  kv[0] = R[0] * jx + R[3] * jy + R[6] * jz;
+  kv[1] = R[1] * jx + R[4] * jy + R[7] * jz;
+  kv[2] = R[2] * jx + R[5] * jy + R[8] * jz;
+  if (a.kvec) {
+    a.kvec[3 * g] = kv[0];
+    a.kvec[3 * g + 1] = kv[1];
+    a.kvec[3 * g + 2] = kv[2];
+  }
+  if (ix == 0 && iy == 0 && iz == 0) {
+    a.green[g] = 0;
+    return;
+  }
+  const double k2 = kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2];
+  constexpr int kMaxAlias = 8;
+  double ux[2 * kMaxAlias + 1], uy[2 * kMaxAlias + 1], uz[2 * kMaxAlias + 1];
+  const int na = a.nalias;
+  for (int q = -na; q <= na; q++) {
+    ux[q + na] = pow(sincpi_d(jx / nx + q), 2 * a.order);
+    uy[q + na] = pow(sincpi_d(jy / ny + q), 2 * a.order);
+    uz[q + na] = pow(sincpi_d(jz / nz + q), 2 * a.order);
+  }
+  double num = 0, d1 = 0, d2 = 0, chi = 0;
+  for (int px = -na; px <= na; px++) {
+    const double mx = jx + px * nx;
+    for (int py = -na; py <= na; py++) {
+      const double my = jy + py * ny;
+      for (int pz = -na; pz <= na; pz++) {
+        const double mz = jz + pz * nz;
+        if (fabs(mx) < 1e-16 && fabs(my) < 1e-16 && fabs(mz) < 1e-16)
+          continue;
+        const double kpx = R[0] * mx + R[3] * my + R[6] * mz;
+        const double kpy = R[1] * mx + R[4] * my + R[7] * mz;
+        const double kpz = R[2] * mx + R[5] * my + R[8] * mz;
+        const double kp2 = kpx * kpx + kpy * kpy + kpz * kpz;
+        const double u2 = ux[px + na] * uy[py + na] * uz[pz + na];
+        const double gg = 4 * M_PI / kp2 * exp(-kp2 * a.inv_4eta2);
+        if (a.ik) {
+          num += gg * u2 * (kv[0] * kpx + kv[1] * kpy + kv[2] * kpz);
+          d1 += u2;
+        } else {
+          num += gg * kp2 * u2;
+          d1 += u2;
+          d2 += u2 * kp2;
+        }
+        chi += gg * gg * kp2;
+      }
+    }
+  }
+  const double den = a.ik ? d1 * d1 * k2 : d1 * d2;
+  a.green[g] = a.inv_v * num / den;
+  chi -= num * num / den;
+  if (a.chi)
+    atomicAdd(a.chi, chi);
+}
+
+cudaError_t launch_p3m_green(mmnb_handle *h)
+{
+  GreenArgs a;
+  for (int d = 0; d < 3; d++)
+    a.n[d] = h->mesh[d];
+  a.nalias = h->cfg.p3m_alias_sum_limit;
+  a.order = h->cfg.p3m_assignment_order;
+  a.ik = h->cfg.p3m_ik_differentiate;
+  // 2 pi inv(latv)^T for the (diagonal) lattice
+  for (int i = 0; i < 9; i++)
+    a.rec[i] = 0;
+  for (int d = 0; d < 3; d++)
+    a.rec[4 * d] = 2 * M_PI * (1.0 / h->box.L[d]);
+  a.inv_v = 1.0 / h->volume;
+  a.inv_4eta2 = 1 / ((2 * h->eta) * (2 * h->eta));
+  a.green = h->d_green;
+  a.kvec = h->d_kvec;
+  a.chi = h->d_energy;  // scratch: reduced chi lands in d_energy[0]
+  const long nk = (long) h->mesh[0] * h->mesh[1] * (h->mesh[2] / 2 + 1);
+  cudaMemsetAsync(h->d_energy, 0, sizeof(double), h->stream);
+  k_green<<<div_up(nk, 128), 128, 0, h->stream>>>(a);
+  return cudaGetLastError();
+}
+
+// ---- FP64 spread / gather -----------------------------------------------------
+
+template <int P>
+__global__ void k_spread_fp64(MeshArgs m, const double *__restrict__ r, const double *__restrict__ q,
+                              const int *__restrict__ mask, double *__restrict__ mesh)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nsite)
+    return;
+  const double qi = q[i];
+  if (!(mask[i] & MMNB_SITE_HAS_Q) || qi == 0)
+    return;
+  const double x = r[3 * i], y = r[3 * i + 1], z = r[3 * i + 2];
+  double W[3][P], ND[3][P];
+  int base[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const double s = m.A[d] * x + m.A[3 + d] * y + m.A[6 + d] * z;
+    base[d] = bspline_weights<P, double>(s, W[d], ND[d]);
+  }
+  int iy_[P], iz_[P];
+#pragma unroll
+  for (int p = 0; p < P; p++) {
+    iy_[p] = wrap_idx(base[1] + p, m.n[1]);
+    iz_[p] = wrap_idx(base[2] + p, m.n[2]);
+  }
+  for (int a = 0; a < P; a++) {
+    const int ix = wrap_idx(base[0] + a, m.n[0]);
+#pragma unroll
+    for (int b = 0; b < P; b++) {
+      const double qw = W[0][a] * W[1][b] * qi;
+      double *row = mesh + ((size_t) ix * m.n[1] + iy_[b]) * m.n[2];
+#pragma unroll
+      for (int c = 0; c < P; c++)
+        atomicAdd(row + iz_[c], qw * W[2][c]);
+    }
+  }
+}
+
+__global__ void k_green_mul(long nk, const double *__restrict__ green, cufftDoubleComplex *__restrict__ meshk,
+                            const double *__restrict__ kvec, cufftDoubleComplex *__restrict__ egk)
+{
+  const long g = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nk)
+    return;
+  const double a = green[g];
+  cufftDoubleComplex v = meshk[g];
+  v.x *= a;
+  v.y *= a;
+  meshk[g] = v;
+  if (egk) {
+    // -ik times the potential: (k im, -k re) per component (src/pppm.c:583-594)
+    for (int d = 0; d < 3; d++) {
+      const double k = kvec[3 * g + d];
+      egk[d * nk + g] = make_cuDoubleComplex(k * v.y, -k * v.x);
+    }
+  }
+}
+
+template <int P>
+__global__ void k_gather_fp64(MeshArgs m, const double *__restrict__ r, const double *__restrict__ mesh,
+                              const double *__restrict__ egrid, size_t nr, double *__restrict__ phi,
+                              double *__restrict__ evec)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nsite)
+    return;
+  const double x = r[3 * i], y = r[3 * i + 1], z = r[3 * i + 2];
+  double W[3][P], ND[3][P];
+  int base[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const double s = m.A[d] * x + m.A[3 + d] * y + m.A[6 + d] * z;
+    base[d] = bspline_weights<P, double>(s, W[d], ND[d]);
+  }
+  int iy_[P], iz_[P];
+#pragma unroll
+  for (int p = 0; p < P; p++) {
+    iy_[p] = wrap_idx(base[1] + p, m.n[1]);
+    iz_[p] = wrap_idx(base[2] + p, m.n[2]);
+  }
+  double ph = 0, gx = 0, gy = 0, gz = 0;
+  for (int a = 0; a < P; a++) {
+    const int ix = wrap_idx(base[0] + a, m.n[0]);
+#pragma unroll
+    for (int b = 0; b < P; b++) {
+      const size_t rowoff = ((size_t) ix * m.n[1] + iy_[b]) * m.n[2];
+      const double wxy = W[0][a] * W[1][b];
+#pragma unroll
+      for (int c = 0; c < P; c++) {
+        const size_t k = rowoff + iz_[c];
+        const double pv = __ldg(mesh + k);
+        ph += wxy * W[2][c] * pv;
+        if (egrid) {
+          const double ww = wxy * W[2][c];
+          gx += ww * __ldg(egrid + k);
+          gy += ww * __ldg(egrid + nr + k);
+          gz += ww * __ldg(egrid + 2 * nr + k);
+        } else {
+          gx += ND[0][a] * W[1][b] * W[2][c] * pv;
+          gy += W[0][a] * ND[1][b] * W[2][c] * pv;
+          gz += wxy * ND[2][c] * pv;
+        }
+      }
+    }
+  }
+  phi[i] += ph;
+  if (egrid) {
+    evec[3 * i] += gx;
+    evec[3 * i + 1] += gy;
+    evec[3 * i + 2] += gz;
+  } else {
+    // E = A^T (-grad_s phi)  (left_operate, include/cart.h:28-36)
+    evec[3 * i] += gx * m.A[0] + gy * m.A[1] + gz * m.A[2];
+    evec[3 * i + 1] += gx * m.A[3] + gy * m.A[4] + gz * m.A[5];
+    evec[3 * i + 2] += gx * m.A[6] + gy * m.A[7] + gz * m.A[8];
+  }
+}
+
+static MeshArgs mesh_args(mmnb_handle *h)
+{
+  MeshArgs m;
+  for (int d = 0; d < 3; d++)
+    m.n[d] = h->mesh[d];
+  for (int i = 0; i < 9; i++)
+    m.A[i] = 0;
+  // inverse of the diagonal lattice as the reference's inverse() computes it,
+  // rows scaled by the mesh size (src/pppm.c:428, 523-525)
+  const double xx = h->box.L[0], yy = h->box.L[1], zz = h->box.L[2];
+  const double det = xx * yy * zz;
+  const double id = 1.0 / det;
+  m.A[0] = id * (yy * zz) * h->mesh[0];
+  m.A[4] = id * (xx * zz) * h->mesh[1];
+  m.A[8] = id * (xx * yy) * h->mesh[2];
+  m.nsite = h->nsite;
+  return m;
+}
+
+template <int P>
+static cudaError_t p3m_fp64_p(mmnb_handle *h, const double *d_r)
+{
+  const MeshArgs m = mesh_args(h);
+  const size_t nr = (size_t) h->mesh[0] * h->mesh[1] * h->mesh[2];
+  const long nk = (long) h->mesh[0] * h->mesh[1] * (h->mesh[2] / 2 + 1);
+  cudaError_t e = cudaMemsetAsync(h->d_mesh, 0, sizeof(double) * nr, h->stream);
+  if (e != cudaSuccess)
+    return e;
+  k_spread_fp64<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->d_q, h->d_mask, h->d_mesh);
+  timing_mark(h, "p3m_spread");
+  if (cufftExecD2Z(h->plan_r2c, h->d_mesh, h->d_meshk) != CUFFT_SUCCESS)
+    return cudaErrorUnknown;
+  const bool ik = h->cfg.p3m_ik_differentiate != 0;
+  k_green_mul<<<div_up(nk, 256), 256, 0, h->stream>>>(nk, h->d_green, h->d_meshk, h->d_kvec,
+                                                      ik ? h->d_egridk : nullptr);
+  if (ik)
+    for (int d = 0; d < 3; d++)
+      if (cufftExecZ2D(h->plan_c2r, h->d_egridk + d * nk, h->d_egrid + d * nr) != CUFFT_SUCCESS)
+        return cudaErrorUnknown;
+  if (cufftExecZ2D(h->plan_c2r, h->d_meshk, h->d_mesh) != CUFFT_SUCCESS)
+    return cudaErrorUnknown;
+  timing_mark(h, "p3m_fft");
+  k_gather_fp64<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->d_mesh, ik ? h->d_egrid : nullptr,
+                                                                 nr, h->d_phi, h->d_evec);
+  timing_mark(h, "p3m_gather");
+  return cudaGetLastError();
+}
+
+cudaError_t launch_p3m_fp64(mmnb_handle *h, const double *d_r)
+{
+  switch (h->cfg.p3m_assignment_order) {
+  case 2: return p3m_fp64_p<2>(h, d_r);
+  case 3: return p3m_fp64_p<3>(h, d_r);
+  case 4: return p3m_fp64_p<4>(h, d_r);
+  case 5: return p3m_fp64_p<5>(h, d_r);
+  case 6: return p3m_fp64_p<6>(h, d_r);
+  case 7: return p3m_fp64_p<7>(h, d_r);
+  default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace mmnb

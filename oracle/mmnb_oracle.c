@@ -240,6 +240,24 @@ static void pset_dump(const pset *p, int *out)
     }
 }
 
+int orc_pairset_demo(int n, int nadd, const int *adds, int *cnt, int *rows, int *exists)
+{
+  pset *p = pset_new(n);
+  int i, j;
+  for (i = 0; i < nadd; i++)
+    pset_add(p, adds[2 * i], adds[2 * i + 1]);
+  pset_sort_unique(p);
+  for (i = 0; i < n; i++) {
+    cnt[i] = p->cnt[i];
+    for (j = 0; j < p->cnt[i] && j < n; j++)
+      rows[i * n + j] = p->row[i][j];
+    for (j = 0; j < n; j++)
+      exists[i * n + j] = pset_has(p, i, j);
+  }
+  pset_free(p);
+  return 0;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Boxes: cubic (type 1) and orthorhombic (type 2), include/bcondtype.h:8. */
 

@@ -131,6 +131,7 @@ class OracleLib:
         L.orc_eleclj_nbrlist.restype = _vp
         L.orc_eleclj_nbrlist.argtypes = [_vp]
         L.orc_eleclj_delete.argtypes = [_vp]
+        L.orc_pairset_demo.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _ip, _ip]
 
     # --- component entry points -------------------------------------------
     def chebyshev(self, rc, eta):
@@ -160,6 +161,15 @@ class OracleLib:
         self.lib.orc_p3m_field(h, _d(r), _d(q), _d(phi), _d(evec))
         self.lib.orc_p3m_delete(h)
         return phi, evec, tuple(int(x) for x in ngrid), chi.value
+
+    def pairset(self, n, adds):
+        """Rows and membership matrix of a PairBinary built from ``adds``."""
+        adds = _i32(adds)
+        cnt = np.zeros(n, dtype=np.int32)
+        rows = np.full((n, n), -1, dtype=np.int32)
+        ex = np.zeros((n, n), dtype=np.int32)
+        self.lib.orc_pairset_demo(n, len(adds), _i(adds), _i(cnt), _i(rows), _i(ex))
+        return [list(rows[i, :cnt[i]]) for i in range(n)], ex
 
     def nbrlist(self, ngroup, cutoff, width, box, bctype=1):
         return NbrList(self, self.lib.orc_nbrlist_new(ngroup, cutoff, width, bctype,

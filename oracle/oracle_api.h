@@ -96,6 +96,11 @@ double orc_eleclj_nlw(void *h);
 void *orc_eleclj_nbrlist(void *h);
 void orc_eleclj_delete(void *h);
 
+/* Pair-set semantics (src/pbin.c:41-137): add the 2*nadd pairs in order, sort
+   and dedupe the rows, then report each row (cnt[i] entries in rows[i*n ...])
+   and the n*n membership matrix. */
+int orc_pairset_demo(int n, int nadd, const int *adds, int *cnt, int *rows, int *exists);
+
 #ifdef __cplusplus
 }
 #endif

@@ -491,4 +491,23 @@ void orc_eleclj_delete(void *hp)
   delete h;
 }
 
+int orc_pairset_demo(int n, int nadd, const int *adds, int *cnt, int *rows, int *exists)
+{
+  struct PairBinary *p = PairBinary_new(n);
+  for (int i = 0; i < nadd; i++)
+    PairBinary_add(p, adds[2 * i], adds[2 * i + 1]);
+  PairBinary_init(p);
+  const int *nn = PairBinary_number_of_elements(p);
+  int *const *t = PairBinary_elements(p);
+  for (int i = 0; i < n; i++) {
+    cnt[i] = nn[i];
+    for (int j = 0; j < nn[i] && j < n; j++)
+      rows[i * n + j] = t[i][j];
+    for (int j = 0; j < n; j++)
+      exists[i * n + j] = PairBinary_exists(p, i, j);
+  }
+  PairBinary_delete(p);
+  return 0;
+}
+
 } /* extern "C" */
