@@ -168,11 +168,19 @@ int mmnb_get_cells(mmnb_handle *h, int *cell_of_group, int *ncell_per_dim);
 /* Number of list rebuilds so far and number of evaluations. */
 int mmnb_get_counters(mmnb_handle *h, long *rebuilds, long *evaluations);
 
+/* Number of this library's kernels launched on the handle's stream so far
+   (library kernels such as cuFFT's are not counted). */
+int mmnb_get_launches(mmnb_handle *h, long *launches);
+
 /* Derived settings: rc, neighbour-list width, eta, P3M mesh (0 if unused). */
 int mmnb_get_settings(mmnb_handle *h, double *rc, double *nlw, double *eta, int mesh[3]);
 
-/* Per-kernel device time (ms) of the last mmnb_compute, when timing is on.
-   Names are written as a comma-separated list into names (size cap). */
+/* Stage timing with CUDA events on the handle's stream.  mmnb_set_timing
+   clears the record and turns it on or off; while on, every evaluation
+   records one event per stage.  mmnb_get_timing synchronises the stream and
+   writes each stage's mean device time per evaluation (ms) into ms[0..nmax)
+   and the stage names, comma-separated, into names (size cap); it returns the
+   number of stages (negative status on error). */
 int mmnb_set_timing(mmnb_handle *h, int on);
 int mmnb_get_timing(mmnb_handle *h, double *ms, int nmax, char *names, int cap);
 

@@ -334,7 +334,16 @@ int setup_p3m(mmnb_handle *h)
   int s;
   if ((s = dalloc(h, &h->d_green, nk)) || (s = dalloc(h, &h->d_kvec, 3 * nk)))
     return s;
-  if (c.precision == MMNB_FP64 || c.p3m_ik_differentiate) {
+  if (c.precision == MMNB_MIXED) {
+    if ((s = dalloc(h, &h->d_mesh_fx, nr)) || (s = dalloc(h, &h->d_mesh32, nr)) ||
+        (s = dalloc(h, &h->d_meshk32, nk)) || (s = dalloc(h, &h->d_green32, nk)))
+      return s;
+    CK(cudaMemset(h->d_mesh_fx, 0, sizeof(unsigned long long) * nr));
+    CKFFT(cufftPlan3d(&h->plan_r2c32, h->mesh[0], h->mesh[1], h->mesh[2], CUFFT_R2C));
+    CKFFT(cufftPlan3d(&h->plan_c2r32, h->mesh[0], h->mesh[1], h->mesh[2], CUFFT_C2R));
+    CKFFT(cufftSetStream(h->plan_r2c32, h->stream));
+    CKFFT(cufftSetStream(h->plan_c2r32, h->stream));
+  } else {
     if ((s = dalloc(h, &h->d_mesh, nr * (c.p3m_ik_differentiate ? 1 : 1))) || (s = dalloc(h, &h->d_meshk, nk)))
       return s;
     CKFFT(cufftPlan3d(&h->plan_r2c, h->mesh[0], h->mesh[1], h->mesh[2], CUFFT_D2Z));
@@ -346,6 +355,8 @@ int setup_p3m(mmnb_handle *h)
         return s;
   }
   CK(launch_p3m_green(h));
+  if (c.precision == MMNB_MIXED)
+    CK(launch_green32(h));
   double chi = 0;
   CK(cudaMemcpyAsync(&chi, h->d_energy, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
@@ -364,7 +375,7 @@ void free_all(mmnb_handle *h)
                   h->d_phi, h->d_evec, h->d_ljf, h->d_lj_part, h->d_elec_part, h->d_energy, h->d_r, h->d_f,
                   h->d_mesh, h->d_meshk, h->d_green, h->d_kvec, h->d_egrid, h->d_egridk, h->d_mesh32,
                   h->d_meshk32, h->d_green32, h->d_mesh_fx, h->d_kint, h->d_kvecs, h->d_ak, h->d_skc,
-                  h->mx.site_xyzq, h->mx.site_lj, h->mx.site_mask, h->mx.anchor, h->mx.acc};
+                  h->mx.site, h->mx.par, h->mx.anchor, h->mx.lj, h->mx.acc, h->d_ep_part};
   for (void *p : ptrs)
     if (p)
       cudaFree(p);
@@ -382,7 +393,7 @@ void free_all(mmnb_handle *h)
     cufftDestroy(h->plan_r2c32);
   if (h->plan_c2r32)
     cufftDestroy(h->plan_c2r32);
-  for (auto e : h->timing.ev)
+  for (auto e : h->timing.pool)
     cudaEventDestroy(e);
 }
 
@@ -392,13 +403,18 @@ namespace mmnb {
 
 void timing_mark(mmnb_handle *h, const char *name)
 {
-  if (!h->timing.on)
+  Timing &t = h->timing;
+  if (!t.on)
     return;
-  cudaEvent_t e;
-  cudaEventCreate(&e);
-  cudaEventRecord(e, h->stream);
-  h->timing.ev.push_back(e);
-  h->timing.names.push_back(name);
+  if (t.used == t.pool.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess)
+      return;
+    t.pool.push_back(e);
+  }
+  cudaEventRecord(t.pool[t.used], h->stream);
+  t.names.push_back(name);
+  t.used++;
 }
 
 }  // namespace mmnb
@@ -497,6 +513,9 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
     return fail(h, MMNB_ERR_ARG, "neighbor_list_width must be >= 0");
   h->rhi2 = sq(h->rc);
   h->rlo2 = sq(h->rc - c->smoothing_width);
+  h->inv_sw = h->rhi2 > h->rlo2 ? 1.0 / (h->rhi2 - h->rlo2) : 0.0;
+  if (c->precision == MMNB_MIXED && c->use_p3m && c->p3m_ik_differentiate)
+    return fail(h, MMNB_ERR_UNSUPPORTED, "the mixed form differentiates P3M in real space only");
   // Ewald parameter (src/eleclj.cpp:189-239)
   h->eta = c->ewald_screening;
   if (c->include_kspace && c->use_p3m) {
@@ -538,7 +557,8 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
   if (c->device >= 0)
     CK(cudaSetDevice(c->device));
   CK(cudaGetDevice(&h->dev));
-  CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+  h->stream = h->own_stream;
   int s;
   std::vector<int> gvec(h->group);
   if ((s = upload(h, &h->d_group, gvec)) || (s = upload(h, &h->d_excl_ptr, h->excl_ptr)) ||
@@ -566,12 +586,22 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
       (s = dalloc(h, &h->d_site_of_slot, nslot)))
     return s;
   h->elec_blocks = div_up(nsite, 256);
+  h->lj_pair_blocks = pair_blocks(h);
+  h->lj_excl_blocks = excl_blocks(h);
+  const size_t nlj = (size_t) h->lj_pair_blocks + h->lj_excl_blocks;
   if ((s = dalloc(h, &h->d_phi, nsite)) || (s = dalloc(h, &h->d_evec, 3 * (size_t) nsite)) ||
-      (s = dalloc(h, &h->d_ljf, 3 * (size_t) nsite)) || (s = dalloc(h, &h->d_lj_part, (size_t) ngroup + nsite)) ||
+      (s = dalloc(h, &h->d_ljf, 3 * (size_t) nsite)) || (s = dalloc(h, &h->d_lj_part, nlj)) ||
       (s = dalloc(h, &h->d_elec_part, h->elec_blocks)) || (s = dalloc(h, &h->d_energy, 8)) ||
       (s = dalloc(h, &h->d_r, 3 * (size_t) nsite)) || (s = dalloc(h, &h->d_f, 3 * (size_t) nsite)))
     return s;
-  CK(cudaMemset(h->d_lj_part, 0, sizeof(double) * ((size_t) ngroup + nsite)));
+  CK(cudaMemset(h->d_lj_part, 0, sizeof(double) * nlj));
+  if (c->precision == MMNB_MIXED) {
+    if ((s = dalloc(h, &h->mx.site, nslot)) || (s = dalloc(h, &h->mx.par, nslot)) ||
+        (s = dalloc(h, &h->mx.anchor, ngroup)) || (s = dalloc(h, &h->mx.lj, ngroup)) ||
+        (s = dalloc(h, &h->mx.acc, (size_t) nsite * kAccStride)) || (s = dalloc(h, &h->d_ep_part, h->lj_pair_blocks)))
+      return s;
+    CK(cudaMemset(h->mx.acc, 0, sizeof(long long) * nsite * kAccStride));
+  }
   CK(cudaMallocHost((void **) &h->h_f, sizeof(double) * 3 * (size_t) nsite));
   CK(cudaMallocHost((void **) &h->h_out, sizeof(double) * 16));
   if ((s = setup_cells(h)))
@@ -604,8 +634,8 @@ int mmnb_create(const mmnb_config *c, int nsite, int ngroup, const int *group, i
   if (s) {
     g_create_error = h->err;
     free_all(h);
-    if (h->stream)
-      cudaStreamDestroy(h->stream);
+    if (h->own_stream)
+      cudaStreamDestroy(h->own_stream);
     delete h;
     return s;
   }
@@ -644,12 +674,15 @@ int mmnb_set_params(mmnb_handle *h, const int *site_mask, const double *q, const
   const int n = h->nsite;
   std::vector<double> rs(n, 0.0);
   h->any_q = h->any_lj = h->has_rscreen = false;
+  h->lj_on_anchors_only = true;
   double qsum = 0;
   for (int i = 0; i < n; i++) {
     if (site_mask[i] & MMNB_SITE_HAS_Q)
       h->any_q = true;
     if (site_mask[i] & MMNB_SITE_HAS_LJ) {
       h->any_lj = true;
+      if (h->group[2 * h->group_of_site[i]] != i)
+        h->lj_on_anchors_only = false;
       if (!(sig[i] > 0) || eps[i] < 0)
         return fail(h, MMNB_ERR_ARG, "LJ sites need sigma > 0 and epsilon >= 0");
     }
@@ -695,6 +728,13 @@ int mmnb_set_params(mmnb_handle *h, const int *site_mask, const double *q, const
       h->totA += bb * s6;
     }
   update_energy_constants(h, qsum);
+  // rigid-water topology: every group [O(q, LJ), H(q), H(q)], nothing else
+  h->water = h->G == 3 && !h->has_rscreen && !h->any_gexcl;
+  for (int g = 0; g < h->ngroup && h->water; g++) {
+    const int a = h->group[2 * g];
+    h->water = h->group[2 * g + 1] - a == 3 && site_mask[a] == (MMNB_SITE_HAS_Q | MMNB_SITE_HAS_LJ) &&
+               site_mask[a + 1] == MMNB_SITE_HAS_Q && site_mask[a + 2] == MMNB_SITE_HAS_Q;
+  }
   h->params_set = true;
   return MMNB_OK;
 }
@@ -705,29 +745,45 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
     return fail(h, MMNB_ERR_ARG, "null handle or positions");
   if (!h->params_set)
     return fail(h, MMNB_ERR_STATE, "mmnb_set_params has not been called");
-  if (h->cfg.precision == MMNB_MIXED)
-    return fail(h, MMNB_ERR_UNSUPPORTED, "mixed precision is not available in this build");
+  const bool mixed = h->cfg.precision == MMNB_MIXED;
   double *energy = d_energy ? d_energy : h->d_energy;
   timing_mark(h, "start");
   CK(launch_gather_anchors(h, d_r));
   CK(launch_rebuild_decide(h, h->force_rebuild_next));
   CK(launch_build_list(h));
   timing_mark(h, "nbrlist");
-  CK(launch_sort_sites(h, d_r));
+  if (mixed || !h->cfg.include_rspace) {
+    // FP64 site arrays collect the terms the fixed-point sums do not hold
+    CK(cudaMemsetAsync(h->d_phi, 0, sizeof(double) * h->nsite, h->stream));
+    CK(cudaMemsetAsync(h->d_evec, 0, sizeof(double) * 3 * h->nsite, h->stream));
+    CK(cudaMemsetAsync(h->d_ljf, 0, sizeof(double) * 3 * h->nsite, h->stream));
+  }
+  if (mixed)
+    CK(launch_prep_mixed(h, d_r));
+  else
+    CK(launch_sort_sites(h, d_r));
+  timing_mark(h, "sort_sites");
+  h->used_water = false;
   if (h->cfg.include_rspace) {
-    CK(launch_rspace_fp64(h));
+    if (mixed && h->water && !h->want_fields) {
+      CK(launch_rspace_water(h));
+      h->used_water = true;
+    } else if (mixed) {
+      CK(launch_rspace_mixed(h));
+    } else {
+      CK(launch_rspace_fp64(h));
+    }
     timing_mark(h, "rspace_pair");
     CK(launch_exclusions(h, d_r));
     timing_mark(h, "rspace_excl");
   } else {
-    CK(cudaMemsetAsync(h->d_phi, 0, sizeof(double) * h->nsite, h->stream));
-    CK(cudaMemsetAsync(h->d_evec, 0, sizeof(double) * 3 * h->nsite, h->stream));
-    CK(cudaMemsetAsync(h->d_ljf, 0, sizeof(double) * 3 * h->nsite, h->stream));
-    CK(cudaMemsetAsync(h->d_lj_part, 0, sizeof(double) * (h->ngroup + h->nsite), h->stream));
+    CK(cudaMemsetAsync(h->d_lj_part, 0, sizeof(double) * (h->lj_pair_blocks + h->lj_excl_blocks), h->stream));
+    if (mixed)
+      CK(cudaMemsetAsync(h->mx.acc, 0, sizeof(long long) * h->nsite * kAccStride, h->stream));
   }
   if (h->any_q && h->cfg.include_kspace) {
     if (h->p3m)
-      CK(launch_p3m_fp64(h, d_r));
+      CK(mixed ? launch_p3m_mixed(h, d_r) : launch_p3m_fp64(h, d_r));
     else if (h->kspace)
       CK(launch_kspace(h, d_r));
     timing_mark(h, "kspace");
@@ -746,16 +802,12 @@ int mmnb_compute(mmnb_handle *h, const double *r, double *f, double *u, mmnb_ene
     return fail(h, MMNB_ERR_ARG, "null handle or positions");
   const size_t n3 = 3 * (size_t) h->nsite;
   for (int attempt = 0; attempt < 2; attempt++) {
-    if (h->timing.on) {
-      for (auto ev : h->timing.ev)
-        cudaEventDestroy(ev);
-      h->timing.ev.clear();
-      h->timing.names.clear();
-    }
     CK(cudaMemcpyAsync(h->d_r, r, sizeof(double) * n3, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemsetAsync(h->d_f, 0, sizeof(double) * n3, h->stream));
     CK(cudaMemsetAsync(h->d_flags + kFlagOverflow, 0, sizeof(int), h->stream));
+    h->want_fields = phi || evec;
     const int s = mmnb_compute_device(h, h->d_r, h->d_f, h->d_energy);
+    h->want_fields = false;
     if (s)
       return s;
     CK(cudaMemcpyAsync(h->h_f, h->d_f, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->stream));
@@ -787,14 +839,6 @@ int mmnb_compute(mmnb_handle *h, const double *r, double *f, double *u, mmnb_ene
       e->lj = h->h_out[1];
       e->lj_correction = h->h_out[2];
       e->total = h->h_out[3];
-    }
-    if (h->timing.on) {
-      h->timing.ms.clear();
-      for (size_t k = 1; k < h->timing.ev.size(); k++) {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, h->timing.ev[k - 1], h->timing.ev[k]);
-        h->timing.ms.push_back(ms);
-      }
     }
     return MMNB_OK;
   }
@@ -830,6 +874,8 @@ int mmnb_scale(mmnb_handle *h, double s)
     const long nk = (long) h->mesh[0] * h->mesh[1] * (h->mesh[2] / 2 + 1);
     k_scale_green<<<div_up(nk, 256), 256, 0, h->stream>>>(nk, s, h->d_green, h->d_kvec);
     CK(cudaGetLastError());
+    if (h->cfg.precision == MMNB_MIXED)
+      CK(launch_green32(h));
   }
   if (h->kspace && (st = setup_kspace(h)))
     return st;
@@ -850,7 +896,8 @@ int mmnb_set_stream(mmnb_handle *h, void *stream)
 {
   if (!h)
     return MMNB_ERR_ARG;
-  h->stream = (cudaStream_t) stream;
+  CK(cudaStreamSynchronize(h->stream));
+  h->stream = stream ? (cudaStream_t) stream : h->own_stream;
   if (h->plan_r2c)
     CKFFT(cufftSetStream(h->plan_r2c, h->stream));
   if (h->plan_c2r)
@@ -918,6 +965,14 @@ int mmnb_get_counters(mmnb_handle *h, long *rebuilds, long *evaluations)
   return MMNB_OK;
 }
 
+int mmnb_get_launches(mmnb_handle *h, long *launches)
+{
+  if (!h || !launches)
+    return MMNB_ERR_ARG;
+  *launches = h->launches;
+  return MMNB_OK;
+}
+
 int mmnb_get_settings(mmnb_handle *h, double *rc, double *nlw, double *eta, int mesh[3])
 {
   if (!h)
@@ -938,28 +993,54 @@ int mmnb_set_timing(mmnb_handle *h, int on)
 {
   if (!h)
     return MMNB_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
   h->timing.on = on != 0;
+  h->timing.used = 0;
+  h->timing.names.clear();
   return MMNB_OK;
 }
 
 int mmnb_get_timing(mmnb_handle *h, double *ms, int nmax, char *names, int cap)
 {
   if (!h)
-    return MMNB_ERR_ARG;
-  const int n = (int) h->timing.ms.size();
+    return -MMNB_ERR_ARG;
+  Timing &t = h->timing;
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess)
+    return -MMNB_ERR_CUDA;
+  std::vector<std::string> order;
+  std::vector<double> total;
+  int nevals = 0;
+  for (size_t k = 0; k < t.used; k++) {
+    if (t.names[k] == "start") {
+      nevals++;
+      continue;
+    }
+    if (k == 0)
+      continue;
+    float dt = 0;
+    cudaEventElapsedTime(&dt, t.pool[k - 1], t.pool[k]);
+    size_t i = 0;
+    while (i < order.size() && order[i] != t.names[k])
+      i++;
+    if (i == order.size()) {
+      order.push_back(t.names[k]);
+      total.push_back(0);
+    }
+    total[i] += dt;
+  }
   std::string all;
-  for (int k = 0; k < n; k++) {
-    if (ms && k < nmax)
-      ms[k] = h->timing.ms[k];
-    if (k)
+  for (size_t i = 0; i < order.size(); i++) {
+    if (ms && (int) i < nmax)
+      ms[i] = nevals ? total[i] / nevals : 0;
+    if (i)
       all += ",";
-    all += h->timing.names[k + 1];
+    all += order[i];
   }
   if (names && cap > 0) {
     strncpy(names, all.c_str(), cap - 1);
     names[cap - 1] = 0;
   }
-  return n;
+  return (int) order.size();
 }
 
 int mmnb_destroy(mmnb_handle *h)
@@ -969,8 +1050,8 @@ int mmnb_destroy(mmnb_handle *h)
   if (h->stream)
     cudaStreamSynchronize(h->stream);
   free_all(h);
-  if (h->stream)
-    cudaStreamDestroy(h->stream);
+  if (h->own_stream)
+    cudaStreamDestroy(h->own_stream);
   delete h;
   return MMNB_OK;
 }

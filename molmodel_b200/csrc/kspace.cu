@@ -78,6 +78,7 @@ cudaError_t launch_kspace(mmnb_handle *h, const double *d_r)
   k_kspace_structure<<<h->nk, kKThreads, 0, h->stream>>>(h->nsite, h->nk, d_r, h->d_q, h->d_kvecs, h->d_skc);
   k_kspace_field<<<div_up(h->nsite, 128), 128, 0, h->stream>>>(h->nsite, h->nk, d_r, h->d_kvecs, h->d_ak,
                                                                h->d_skc, h->d_phi, h->d_evec);
+  h->launches += 2;
   return cudaGetLastError();
 }
 

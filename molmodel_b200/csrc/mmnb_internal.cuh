@@ -38,22 +38,29 @@ struct CellGeom {
   double c2;        // (cutoff + width)^2
 };
 
+// Fixed-point scale of the mixed form's accumulators: 2^32 units per unit of
+// potential, field or force (range +-2^31, resolution 2.3e-10).
+constexpr double kFxScale = 4294967296.0;
+constexpr double kFxInv = 1.0 / 4294967296.0;
+constexpr int kAccStride = 8;  // phi, Ex, Ey, Ez, Lx, Ly, Lz, (pad) per site
+
 // Device buffers of the mixed-precision form.
 struct MixedBufs {
-  float4 *site_xyzq = nullptr;   // sorted, padded: offset from anchor (xyz) + charge (w)
-  float2 *site_lj = nullptr;     // sorted, padded: sigma, sqrt(epsilon)
-  int *site_mask = nullptr;      // sorted, padded
-  double *anchor = nullptr;      // sorted anchors (3 per group), wrapped into the box
-  long long *acc = nullptr;      // fixed-point accumulators: per sorted site 7 values
-  float *cheb32 = nullptr;       // unused placeholder for an FP32 table
-  int *mesh_fx = nullptr;        // unused
+  float4 *site = nullptr;        // sorted, padded slots: offset from the anchor (xyz), charge (w)
+  float4 *par = nullptr;         // sorted, padded slots: sigma, sqrt(epsilon), rscreen, mask bits
+  double4 *anchor = nullptr;     // sorted groups: anchor position (FP64)
+  float2 *lj = nullptr;          // sorted groups: anchor sigma, sqrt(epsilon)
+  long long *acc = nullptr;      // per site (original order), kAccStride fixed-point values
 };
 
+// Stage timing with CUDA events recorded on the handle's stream.  Each
+// evaluation starts with a "start" mark; a stage's time is the interval from
+// the previous mark to its own.
 struct Timing {
   bool on = false;
-  std::vector<cudaEvent_t> ev;
-  std::vector<std::string> names;
-  std::vector<double> ms;
+  std::vector<cudaEvent_t> pool;   // reused between resets
+  std::vector<std::string> names;  // one per recorded mark
+  size_t used = 0;
 };
 
 }  // namespace mmnb
@@ -62,15 +69,20 @@ struct mmnb_handle {
   mmnb_config cfg{};
   int nsite = 0, ngroup = 0, maxgs = 1, G = 1;   // G: padded sites per group slot
   int dev = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;       // stream every launch goes to
+  cudaStream_t own_stream = nullptr;   // created by mmnb_create, destroyed by mmnb_destroy
   std::string err;
 
   // derived settings
-  double rc = 0, nlw = 0, eta = 0, rlo2 = 0, rhi2 = 0;
+  double rc = 0, nlw = 0, eta = 0, rlo2 = 0, rhi2 = 0, inv_sw = 0;  // inv_sw = 1/(rhi2 - rlo2)
   mmnb::Box box{};
   double volume = 0, min_diameter = 0;
   bool params_set = false, any_q = false, any_lj = false, has_rscreen = false;
   bool any_gexcl = false, use_14 = false;
+  bool lj_on_anchors_only = false;   // every LJ site is its group's first site (rigid water)
+  bool water = false;                // every group is [O(q, LJ), H(q), H(q)] with no screening or group exclusions
+  bool want_fields = false;          // this evaluation must produce per-site potential and field
+  bool used_water = false;           // the last evaluation ran the water kernel
   double totA = 0, totB = 0, lj_correction = 0, neutral_b = 0;
 
   // host topology
@@ -114,6 +126,7 @@ struct mmnb_handle {
   int *d_flags = nullptr;            // mmnb::kFlagCount ints
   int *h_flags = nullptr;            // pinned mirror
   long rebuilds = 0, evals = 0;
+  long launches = 0;                 // kernels of this library launched so far
   bool first = true;
   int force_rebuild_next = 0;
 
@@ -124,7 +137,9 @@ struct mmnb_handle {
 
   // outputs (original order)
   double *d_phi = nullptr, *d_evec = nullptr, *d_ljf = nullptr;
-  double *d_lj_part = nullptr;       // per sorted group LJ energy
+  double *d_lj_part = nullptr;       // LJ energy partials: pair-kernel blocks, then exclusion blocks
+  double *d_ep_part = nullptr;       // real-space Coulomb energy partials of the water kernel
+  int lj_pair_blocks = 0, lj_excl_blocks = 0;
   double *d_elec_part = nullptr;     // per block
   int elec_blocks = 0;
   double *d_energy = nullptr;        // 4 doubles
@@ -172,16 +187,58 @@ cudaError_t launch_rebuild_decide(mmnb_handle *h, int force);
 cudaError_t launch_build_list(mmnb_handle *h);
 cudaError_t launch_sort_sites(mmnb_handle *h, const double *d_r);
 cudaError_t launch_rspace_fp64(mmnb_handle *h);
-cudaError_t launch_rspace_mixed(mmnb_handle *h, const double *d_r);
+cudaError_t launch_prep_mixed(mmnb_handle *h, const double *d_r);
+cudaError_t launch_rspace_mixed(mmnb_handle *h);
+cudaError_t launch_rspace_water(mmnb_handle *h);
 cudaError_t launch_exclusions(mmnb_handle *h, const double *d_r);
 cudaError_t launch_p3m_green(mmnb_handle *h);
 cudaError_t launch_p3m_fp64(mmnb_handle *h, const double *d_r);
 cudaError_t launch_p3m_mixed(mmnb_handle *h, const double *d_r);
+cudaError_t launch_green32(mmnb_handle *h);
 cudaError_t launch_kspace(mmnb_handle *h, const double *d_r);
 cudaError_t launch_finalize(mmnb_handle *h, double *d_f, double *d_energy);
+cudaError_t launch_energy(mmnb_handle *h, double *d_energy);
 
 // helpers shared by the .cu files
 void timing_mark(mmnb_handle *h, const char *name);
+int pair_blocks(const mmnb_handle *h);
+int excl_blocks(const mmnb_handle *h);
+
+#ifdef __CUDACC__
+// binary search of key in CSR row `row` (sorted)
+__device__ __forceinline__ bool csr_has(const int *ptr, const int *idx, int row, int key)
+{
+  int lo = ptr[row], hi = ptr[row + 1] - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    const int v = idx[mid];
+    if (key < v)
+      hi = mid - 1;
+    else if (key > v)
+      lo = mid + 1;
+    else
+      return true;
+  }
+  return false;
+}
+
+// anchor displacement with the reference's minimum-image rounding
+__device__ __forceinline__ double anchor_disp(const Box &b, double4 ri, double4 rj, double &x, double &y, double &z,
+                                              double &sx, double &sy, double &sz)
+{
+  x = __dsub_rn(ri.x, rj.x);
+  y = __dsub_rn(ri.y, rj.y);
+  z = __dsub_rn(ri.z, rj.z);
+  sx = __dmul_rn(-b.L[0], floor(__dadd_rn(__dmul_rn(x, b.invL[0]), 0.5)));
+  sy = __dmul_rn(-b.L[1], floor(__dadd_rn(__dmul_rn(y, b.invL[1]), 0.5)));
+  sz = __dmul_rn(-b.L[2], floor(__dadd_rn(__dmul_rn(z, b.invL[2]), 0.5)));
+  x = __dadd_rn(x, sx);
+  y = __dadd_rn(y, sy);
+  z = __dadd_rn(z, sz);
+  return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
+}
+
+#endif
 
 inline int div_up(long a, long b) { return (int) ((a + b - 1) / b); }
 

@@ -311,6 +311,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(BuildArgs a)
 cudaError_t launch_gather_anchors(mmnb_handle *h, const double *d_r)
 {
   k_gather_anchors<<<div_up(h->ngroup, 256), 256, 0, h->stream>>>(d_r, h->d_group, h->ngroup, h->d_anchor);
+  h->launches += 1;
   return cudaGetLastError();
 }
 
@@ -319,6 +320,7 @@ cudaError_t launch_rebuild_decide(mmnb_handle *h, int force)
   k_top2<<<h->top2_blocks, kTop2Threads, 0, h->stream>>>(h->d_anchor, h->d_last, h->ngroup, h->d_top2);
   k_decide<<<1, kTop2Threads, 0, h->stream>>>(h->d_top2, h->top2_blocks, h->nlw, h->first ? 1 : 0, force,
                                                h->cfg.rebuild_interval, h->d_flags);
+  h->launches += 2;
   return cudaGetLastError();
 }
 
@@ -353,6 +355,7 @@ cudaError_t launch_build_list(mmnb_handle *h)
   a.nbr_count = h->d_nbr_count;
   a.flags_w = h->d_flags;
   k_build_list<<<div_up(h->ngroup, kBuildWarps), kBuildWarps * 32, 0, h->stream>>>(a);
+  h->launches += 5;
   return cudaGetLastError();
 }
 

@@ -24,21 +24,29 @@ struct MeshArgs {
   int nsite;
 };
 
-// Weights W[p] and negated derivatives ND[p] for mesh points j + lo + p,
-// where s is the particle's mesh coordinate (src/pppm.c:533-557).
-template <int P, typename T>
-__device__ __forceinline__ int bspline_weights(T s, T *W, T *ND)
+// Nearest mesh point and offset of a particle at mesh coordinate s
+// (src/pppm.c:533-548): returns the first of the P assigned points and
+// w = delta + 1/2 in [0, 1].
+template <int P>
+__device__ __forceinline__ int bspline_base(double s, double &w)
 {
   int j;
-  T delta;
+  double delta;
   if (P % 2) {
-    j = (int) floor(s + T(0.5));
-    delta = s - T(j);
+    j = (int) floor(s + 0.5);
+    delta = s - j;
   } else {
     j = (int) floor(s);
-    delta = s - (T(j) + T(0.5));
+    delta = s - (j + 0.5);
   }
-  const T w = delta + T(0.5);
+  w = delta + 0.5;
+  return j - ((P + 1) / 2 - 1);
+}
+
+// Weights W[p] and negated derivatives ND[p] of the points base + p.
+template <int P, typename T>
+__device__ __forceinline__ void bspline_eval(T w, T *W, T *ND)
+{
   T m[P], prev[P];
   m[0] = T(1);
 #pragma unroll
@@ -62,7 +70,15 @@ __device__ __forceinline__ int bspline_weights(T s, T *W, T *ND)
     const T b = i > 0 ? prev[i - 1] : T(0);
     ND[p] = b - a;
   }
-  return j - ((P + 1) / 2 - 1);
+}
+
+template <int P>
+__device__ __forceinline__ int bspline_weights(double s, double *W, double *ND)
+{
+  double w;
+  const int base = bspline_base<P>(s, w);
+  bspline_eval<P, double>(w, W, ND);
+  return base;
 }
 
 __device__ __forceinline__ int wrap_idx(int i, int n)
@@ -198,7 +214,7 @@ __global__ void k_spread_fp64(MeshArgs m, const double *__restrict__ r, const do
 #pragma unroll
   for (int d = 0; d < 3; d++) {
     const double s = m.A[d] * x + m.A[3 + d] * y + m.A[6 + d] * z;
-    base[d] = bspline_weights<P, double>(s, W[d], ND[d]);
+    base[d] = bspline_weights<P>(s, W[d], ND[d]);
   }
   int iy_[P], iz_[P];
 #pragma unroll
@@ -253,7 +269,7 @@ __global__ void k_gather_fp64(MeshArgs m, const double *__restrict__ r, const do
 #pragma unroll
   for (int d = 0; d < 3; d++) {
     const double s = m.A[d] * x + m.A[3 + d] * y + m.A[6 + d] * z;
-    base[d] = bspline_weights<P, double>(s, W[d], ND[d]);
+    base[d] = bspline_weights<P>(s, W[d], ND[d]);
   }
   int iy_[P], iz_[P];
 #pragma unroll
@@ -344,6 +360,7 @@ static cudaError_t p3m_fp64_p(mmnb_handle *h, const double *d_r)
   k_gather_fp64<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->d_mesh, ik ? h->d_egrid : nullptr,
                                                                  nr, h->d_phi, h->d_evec);
   timing_mark(h, "p3m_gather");
+  h->launches += 3;
   return cudaGetLastError();
 }
 
@@ -356,6 +373,183 @@ cudaError_t launch_p3m_fp64(mmnb_handle *h, const double *d_r)
   case 5: return p3m_fp64_p<5>(h, d_r);
   case 6: return p3m_fp64_p<6>(h, d_r);
   case 7: return p3m_fp64_p<7>(h, d_r);
+  default: return cudaErrorInvalidValue;
+  }
+}
+
+// ---- mixed form: FP32 weights, 64-bit fixed-point mesh, FP32 FFT -------------
+//
+// Charge assignment accumulates q w_x w_y w_z in 64-bit fixed point
+// (2^32 units per unit charge), so the mesh, and everything computed from it,
+// is bitwise independent of the order in which sites are spread.
+
+template <int P>
+__global__ void k_spread_mixed(MeshArgs m, const double *__restrict__ r, const double *__restrict__ q,
+                               const int *__restrict__ mask, const int *__restrict__ sorted,
+                               const int *__restrict__ group, int nslot, int G, unsigned long long *__restrict__ mesh)
+{
+  const int sl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sl >= nslot)
+    return;
+  const int g = sorted[sl / G];
+  const int i = group[2 * g] + sl % G;
+  if (i >= group[2 * g + 1] || !(mask[i] & MMNB_SITE_HAS_Q))
+    return;
+  const float qi = (float) q[i];
+  const double x = r[3 * i], y = r[3 * i + 1], z = r[3 * i + 2];
+  float W[3][P], ND[3][P];
+  int base[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    double w;
+    base[d] = bspline_base<P>(m.A[d] * x + m.A[3 + d] * y + m.A[6 + d] * z, w);
+    bspline_eval<P, float>((float) w, W[d], ND[d]);
+  }
+  int iy_[P], iz_[P];
+#pragma unroll
+  for (int p = 0; p < P; p++) {
+    iy_[p] = wrap_idx(base[1] + p, m.n[1]);
+    iz_[p] = wrap_idx(base[2] + p, m.n[2]);
+  }
+  for (int a = 0; a < P; a++) {
+    const int ix = wrap_idx(base[0] + a, m.n[0]);
+#pragma unroll
+    for (int b = 0; b < P; b++) {
+      const float qw = W[0][a] * W[1][b] * qi;
+      unsigned long long *row = mesh + ((size_t) ix * m.n[1] + iy_[b]) * m.n[2];
+#pragma unroll
+      for (int c = 0; c < P; c++)
+        atomicAdd(row + iz_[c], (unsigned long long) __float2ll_rn(qw * W[2][c] * 4294967296.0f));
+    }
+  }
+}
+
+// fixed-point mesh -> FP32 FFT input; clears the fixed-point mesh for the next step
+__global__ void k_mesh_fx_to_f32(size_t n, unsigned long long *__restrict__ fx, float *__restrict__ out)
+{
+  const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  out[i] = (float) ((double) (long long) fx[i] * kFxInv);
+  fx[i] = 0ull;
+}
+
+__global__ void k_green_mul32(long nk, const float *__restrict__ green, cufftComplex *__restrict__ meshk)
+{
+  const long g = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nk)
+    return;
+  const float a = green[g];
+  cufftComplex v = meshk[g];
+  v.x *= a;
+  v.y *= a;
+  meshk[g] = v;
+}
+
+__global__ void k_green_to_f32(long nk, const double *__restrict__ green, float *__restrict__ out)
+{
+  const long g = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < nk)
+    out[g] = (float) green[g];
+}
+
+template <int P>
+__global__ void k_gather_mixed(MeshArgs m, const double *__restrict__ r, const int *__restrict__ sorted,
+                               const int *__restrict__ group, int nslot, int G, const float *__restrict__ mesh,
+                               long long *__restrict__ acc)
+{
+  const int sl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sl >= nslot)
+    return;
+  const int g = sorted[sl / G];
+  const int i = group[2 * g] + sl % G;
+  if (i >= group[2 * g + 1])
+    return;
+  const double x = r[3 * i], y = r[3 * i + 1], z = r[3 * i + 2];
+  float W[3][P], ND[3][P];
+  int base[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    double w;
+    base[d] = bspline_base<P>(m.A[d] * x + m.A[3 + d] * y + m.A[6 + d] * z, w);
+    bspline_eval<P, float>((float) w, W[d], ND[d]);
+  }
+  int iy_[P], iz_[P];
+#pragma unroll
+  for (int p = 0; p < P; p++) {
+    iy_[p] = wrap_idx(base[1] + p, m.n[1]);
+    iz_[p] = wrap_idx(base[2] + p, m.n[2]);
+  }
+  float ph = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+  for (int a = 0; a < P; a++) {
+    const int ix = wrap_idx(base[0] + a, m.n[0]);
+#pragma unroll
+    for (int b = 0; b < P; b++) {
+      const float *row = mesh + ((size_t) ix * m.n[1] + iy_[b]) * m.n[2];
+      const float wxy = W[0][a] * W[1][b];
+      const float dxy = ND[0][a] * W[1][b];
+      const float xdy = W[0][a] * ND[1][b];
+      float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+      for (int c = 0; c < P; c++) {
+        const float pv = __ldg(row + iz_[c]);
+        s0 = fmaf(W[2][c], pv, s0);
+        s1 = fmaf(ND[2][c], pv, s1);
+      }
+      ph = fmaf(wxy, s0, ph);
+      gx = fmaf(dxy, s0, gx);
+      gy = fmaf(xdy, s0, gy);
+      gz = fmaf(wxy, s1, gz);
+    }
+  }
+  const float A0 = (float) m.A[0], A4 = (float) m.A[4], A8 = (float) m.A[8];
+  long long *o = acc + (size_t) i * kAccStride;
+  o[0] += __float2ll_rn(ph * 4294967296.0f);
+  o[1] += __float2ll_rn(gx * A0 * 4294967296.0f);
+  o[2] += __float2ll_rn(gy * A4 * 4294967296.0f);
+  o[3] += __float2ll_rn(gz * A8 * 4294967296.0f);
+}
+
+cudaError_t launch_green32(mmnb_handle *h)
+{
+  const long nk = (long) h->mesh[0] * h->mesh[1] * (h->mesh[2] / 2 + 1);
+  k_green_to_f32<<<div_up(nk, 256), 256, 0, h->stream>>>(nk, h->d_green, h->d_green32);
+  return cudaGetLastError();
+}
+
+template <int P>
+static cudaError_t p3m_mixed_p(mmnb_handle *h, const double *d_r)
+{
+  const MeshArgs m = mesh_args(h);
+  const size_t nr = (size_t) h->mesh[0] * h->mesh[1] * h->mesh[2];
+  const long nk = (long) h->mesh[0] * h->mesh[1] * (h->mesh[2] / 2 + 1);
+  const int nslot = h->ngroup * h->G;
+  k_spread_mixed<P><<<div_up(nslot, 128), 128, 0, h->stream>>>(m, d_r, h->d_q, h->d_mask, h->d_sorted, h->d_group,
+                                                               nslot, h->G, h->d_mesh_fx);
+  k_mesh_fx_to_f32<<<div_up((long) nr, 256), 256, 0, h->stream>>>(nr, h->d_mesh_fx, h->d_mesh32);
+  timing_mark(h, "p3m_spread");
+  if (cufftExecR2C(h->plan_r2c32, h->d_mesh32, h->d_meshk32) != CUFFT_SUCCESS)
+    return cudaErrorUnknown;
+  k_green_mul32<<<div_up(nk, 256), 256, 0, h->stream>>>(nk, h->d_green32, h->d_meshk32);
+  if (cufftExecC2R(h->plan_c2r32, h->d_meshk32, h->d_mesh32) != CUFFT_SUCCESS)
+    return cudaErrorUnknown;
+  timing_mark(h, "p3m_fft");
+  k_gather_mixed<P><<<div_up(nslot, 128), 128, 0, h->stream>>>(m, d_r, h->d_sorted, h->d_group, nslot, h->G,
+                                                               h->d_mesh32, h->mx.acc);
+  timing_mark(h, "p3m_gather");
+  h->launches += 4;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_p3m_mixed(mmnb_handle *h, const double *d_r)
+{
+  switch (h->cfg.p3m_assignment_order) {
+  case 2: return p3m_mixed_p<2>(h, d_r);
+  case 3: return p3m_mixed_p<3>(h, d_r);
+  case 4: return p3m_mixed_p<4>(h, d_r);
+  case 5: return p3m_mixed_p<5>(h, d_r);
+  case 6: return p3m_mixed_p<6>(h, d_r);
+  case 7: return p3m_mixed_p<7>(h, d_r);
   default: return cudaErrorInvalidValue;
   }
 }

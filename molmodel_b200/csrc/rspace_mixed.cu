@@ -1,0 +1,636 @@
+// Real-space Ewald + Lennard-Jones, mixed-precision form.
+//
+// Same group-pair semantics as the FP64 form (RSpaceEwald, src/rspace.c:413-491):
+// the cutoff test and minimum image use the FP64 anchor positions with the
+// reference's rounding, so the set of evaluated group pairs is the FP64 set.
+// Everything after that is FP32:
+//   * site positions enter as FP32 offsets from their group's anchor, so a
+//     site-pair displacement is (anchor displacement, FP64 -> FP32) plus the
+//     difference of two small offsets: relative precision ~1e-7 at any box
+//     size, although the unwrapped coordinates themselves can be large;
+//   * erfc(eta r) uses Abramowitz & Stegun 7.1.26 (Hastings' rational
+//     approximation, |error| <= 1.5e-7), with exp(-eta^2 r^2) shared with the
+//     field term b1 = (b0 + 2 eta/sqrt(pi) exp(-eta^2 r^2)) / r^2;
+//   * the switch and LJ terms are the FP64 form's formulas in FP32.
+// Each group pair's contribution to each row site (potential, field, LJ
+// force) is summed in FP32 and then converted to 64-bit fixed point
+// (2^32 units per unit) before it is added: integer addition is associative,
+// so the totals do not depend on the list order, on which lane took which
+// pair, or on the reduction order — the forces are bitwise deterministic.
+//
+// Work layout as in the FP64 form: full list, one warp per row group, a
+// ballot-compacted shared-memory queue of in-cutoff partners so every lane
+// evaluates a group pair, and a shared-memory transpose to reduce the lanes'
+// fixed-point totals.
+
+#include "mmnb_internal.cuh"
+
+namespace mmnb {
+
+constexpr int kMxWarps = 4;
+constexpr int kMxQueue = 64;
+constexpr int kNacc = 7;  // phi, E (3), LJ force (3)
+
+// erfc(x) ~= t P(t) exp(-x^2), t = 1/(1 + p x): Hastings' form (Abramowitz &
+// Stegun 7.1.26) with P refitted for relative accuracy (<= 4e-7 for all x >= 0,
+// FP32 Horner included); molmodel_b200/csrc/fit_erfc.py derives the table.
+constexpr float kErfcP = 0.3275911f;
+constexpr float kE0 = 0.185182706f, kE1 = 0.179008603f, kE2 = 0.215395942f, kE3 = -0.00290450454f,
+                kE4 = 0.502499402f, kE5 = -0.455885917f, kE6 = 0.524125457f, kE7 = -0.147421896f;
+
+__device__ __forceinline__ float ex2_approx(float x)
+{
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+__device__ __forceinline__ float rcp_approx(float x)
+{
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// b0 = erfc(eta r)/r and b1 = (b0 + c2 exp(-eta^2 r^2))/r^2 from r^2 and 1/r;
+// nel2 = -eta^2 log2(e)
+__device__ __forceinline__ void ewald_f32(float r2, float rinv, float eta, float nel2, float c2, float &b0,
+                                          float &b1)
+{
+  const float x = eta * (r2 * rinv);
+  const float t = rcp_approx(fmaf(kErfcP, x, 1.f));
+  float p = fmaf(kE7, t, kE6);
+  p = fmaf(p, t, kE5);
+  p = fmaf(p, t, kE4);
+  p = fmaf(p, t, kE3);
+  p = fmaf(p, t, kE2);
+  p = fmaf(p, t, kE1);
+  p = fmaf(p, t, kE0);
+  const float e = ex2_approx(r2 * nel2);
+  b0 = t * p * e * rinv;
+  b1 = fmaf(c2, e, b0) * (rinv * rinv);
+}
+
+struct MixedArgs {
+  int ngroup, rowcap, geometric;
+  Box box;
+  double rhi2;
+  float rlo2, inv_sw, eta, c2, nel2;  // c2 = 2 eta / sqrt(pi), nel2 = -eta^2 log2(e)
+  const float4 *site;           // offset from anchor, charge
+  const float4 *par;            // sigma, sqrt(eps), rscreen, mask bits
+  const double4 *anchor;
+  const int *nbr, *nbr_count, *sorted, *group;
+  const int *gexcl_ptr, *gexcl_idx, *excl_ptr, *excl_idx;
+  long long *acc;               // per site, kAccStride
+  double *lj_part;
+};
+
+__device__ __forceinline__ long long to_fx(float v) { return __float2ll_rn(v * 4294967296.0f); }
+
+// one group pair inside the cutoff: FP32 sums, then fixed point
+template <int G, bool SCREEN, bool GEXCL, bool ANCHOR_LJ>
+__device__ __forceinline__ void pair_mixed(const MixedArgs &a, const float4 (&oi)[G], const float4 (&pi)[G], int gi,
+                                           int si0, int q, float4 da, long long (&fx)[G][kNacc], long long &fe)
+{
+  float4 oj[G], pj[G];
+#pragma unroll
+  for (int k = 0; k < G; k++) {
+    oj[k] = a.site[(size_t) q * G + k];
+    pj[k] = a.par[(size_t) q * G + k];
+  }
+  const float r2a = da.w;
+  float s = 1.f, ds = 0.f;
+  const bool smoothing = r2a > a.rlo2;
+  if (smoothing) {
+    const float z = (r2a - a.rlo2) * a.inv_sw;
+    s = fmaf(fmaf(fmaf(-6.f, z, 15.f), z, -10.f), z * z * z, 1.f);
+    ds = fmaf(fmaf(60.f, z, -120.f), z, 60.f) * z * z * a.inv_sw;
+  }
+  bool gx = false;
+  int sj0 = 0;
+  if (GEXCL) {
+    const int gj = a.sorted[q];
+    gx = csr_has(a.gexcl_ptr, a.gexcl_idx, gi, gj);
+    sj0 = a.group[2 * gj];
+  }
+  float ph[G], ex[G], ey[G], ez[G], lx[G], ly[G], lz[G];
+#pragma unroll
+  for (int k = 0; k < G; k++)
+    ph[k] = ex[k] = ey[k] = ez[k] = lx[k] = ly[k] = lz[k] = 0.f;
+  float tmps = 0.f, u_sum = 0.f;
+#pragma unroll
+  for (int ia = 0; ia < G; ia++) {
+    const int mi = __float_as_int(pi[ia].w);
+    const float cx = da.x + oi[ia].x, cy = da.y + oi[ia].y, cz = da.z + oi[ia].z;
+    float tq = 0.f;  // sum_j q_j b0 before switching, for the switch derivative
+#pragma unroll
+    for (int jb = 0; jb < G; jb++) {
+      const int m = mi & __float_as_int(pj[jb].w);
+      if (!m)
+        continue;
+      if (GEXCL && gx && csr_has(a.excl_ptr, a.excl_idx, si0 + ia, sj0 + jb))
+        continue;
+      const float dx = cx - oj[jb].x, dy = cy - oj[jb].y, dz = cz - oj[jb].z;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      const float rinv = rsqrtf(r2);
+      if (m & MMNB_SITE_HAS_Q) {
+        float b0, b1;
+        ewald_f32(r2, rinv, a.eta, a.nel2, a.c2, b0, b1);
+        if (SCREEN) {
+          const float rs = pi[ia].z + pj[jb].z;
+          if (r2 < rs * rs) {
+            const float inv3 = 1.f / (rs * rs * rs);
+            b0 += fmaf(-0.5f * r2, inv3, 1.5f / rs) - rinv;
+            b1 += inv3 - rinv * rinv * rinv;
+          }
+        }
+        const float qj = oj[jb].w;
+        tq = fmaf(qj, b0, tq);
+        const float qs = qj * s;
+        ph[ia] = fmaf(qs, b0, ph[ia]);
+        const float f = qs * b1;
+        ex[ia] = fmaf(f, dx, ex[ia]);
+        ey[ia] = fmaf(f, dy, ey[ia]);
+        ez[ia] = fmaf(f, dz, ez[ia]);
+      }
+      if (m & MMNB_SITE_HAS_LJ) {
+        const float sg = a.geometric ? pi[ia].x * pj[jb].x : 0.5f * (pi[ia].x + pj[jb].x) * 0.5f * (pi[ia].x + pj[jb].x);
+        const float s6 = sg * sg * sg;
+        const float b = 4.f * pi[ia].y * pj[jb].y * s6;
+        const float aa = b * s6;
+        const float ir2 = rinv * rinv;
+        const float ir6 = ir2 * ir2 * ir2;
+        const float bi6 = b * ir6;
+        const float ai12 = aa * ir6 * ir6;
+        const float du = (12.f * ai12 - 6.f * bi6) * ir2 * s;
+        const float u = ai12 - bi6;
+        tmps += u;
+        u_sum = fmaf(u, s, u_sum);
+        lx[ia] = fmaf(du, dx, lx[ia]);
+        ly[ia] = fmaf(du, dy, ly[ia]);
+        lz[ia] = fmaf(du, dz, lz[ia]);
+      }
+    }
+    tmps = fmaf(oi[ia].w, tq, tmps);
+  }
+  if (smoothing) {
+    const float g = ds * tmps;
+    lx[0] = fmaf(g, da.x, lx[0]);
+    ly[0] = fmaf(g, da.y, ly[0]);
+    lz[0] = fmaf(g, da.z, lz[0]);
+  }
+#pragma unroll
+  for (int k = 0; k < G; k++) {
+    fx[k][0] += to_fx(ph[k]);
+    fx[k][1] += to_fx(ex[k]);
+    fx[k][2] += to_fx(ey[k]);
+    fx[k][3] += to_fx(ez[k]);
+    if (!ANCHOR_LJ || k == 0) {
+      fx[k][4] += to_fx(lx[k]);
+      fx[k][5] += to_fx(ly[k]);
+      fx[k][6] += to_fx(lz[k]);
+    }
+  }
+  fe += to_fx(0.5f * u_sum);
+}
+
+template <int G, bool SCREEN, bool GEXCL, bool ANCHOR_LJ>
+__global__ void __launch_bounds__(kMxWarps * 32) k_pair_mixed(MixedArgs a)
+{
+  __shared__ float4 qda[kMxWarps][kMxQueue];
+  __shared__ int qix[kMxWarps][kMxQueue];
+  constexpr int kCols = G * kNacc + 1;
+  constexpr bool kTranspose = G <= 4;
+  __shared__ long long red[kTranspose ? kMxWarps : 1][kTranspose ? 32 : 1][kTranspose ? kCols : 1];
+  __shared__ long long wlj[kMxWarps];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int p = blockIdx.x * kMxWarps + w;
+  long long fx[G][kNacc];
+#pragma unroll
+  for (int k = 0; k < G; k++)
+#pragma unroll
+    for (int c = 0; c < kNacc; c++)
+      fx[k][c] = 0;
+  long long fe = 0;
+  int gi = 0, si0 = 0, ns = 0;
+  if (p < a.ngroup) {
+    float4 oi[G], pi[G];
+#pragma unroll
+    for (int k = 0; k < G; k++) {
+      oi[k] = a.site[(size_t) p * G + k];
+      pi[k] = a.par[(size_t) p * G + k];
+    }
+    const double4 ai = a.anchor[p];
+    gi = a.sorted[p];
+    si0 = a.group[2 * gi];
+    ns = a.group[2 * gi + 1] - si0;
+    const int cnt = a.nbr_count[p];
+    const int *row = a.nbr + (size_t) p * a.rowcap;
+    const unsigned below = (1u << lane) - 1;
+    int qn = 0;
+    for (int base = 0; base < cnt; base += 32) {
+      const int e = base + lane;
+      bool take = false;
+      int q = 0;
+      float4 da = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (e < cnt) {
+        q = row[e];
+        double x, y, z, sx, sy, sz;
+        const double r2a = anchor_disp(a.box, ai, a.anchor[q], x, y, z, sx, sy, sz);
+        take = r2a <= a.rhi2;
+        da = make_float4((float) x, (float) y, (float) z, (float) r2a);
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, take);
+      if (take) {
+        const int idx = qn + __popc(bal & below);
+        qda[w][idx] = da;
+        qix[w][idx] = q;
+      }
+      qn += __popc(bal);
+      __syncwarp();
+      if (qn >= 32) {
+        pair_mixed<G, SCREEN, GEXCL, ANCHOR_LJ>(a, oi, pi, gi, si0, qix[w][lane], qda[w][lane], fx, fe);
+        __syncwarp();
+        if (lane < qn - 32) {
+          qda[w][lane] = qda[w][lane + 32];
+          qix[w][lane] = qix[w][lane + 32];
+        }
+        __syncwarp();
+        qn -= 32;
+      }
+    }
+    if (lane < qn)
+      pair_mixed<G, SCREEN, GEXCL, ANCHOR_LJ>(a, oi, pi, gi, si0, qix[w][lane], qda[w][lane], fx, fe);
+  }
+  if constexpr (kTranspose) {
+    // transpose reduction: lane c sums column c over the 32 lanes
+#pragma unroll
+    for (int k = 0; k < G; k++)
+#pragma unroll
+      for (int c = 0; c < kNacc; c++)
+        red[w][lane][k * kNacc + c] = fx[k][c];
+    red[w][lane][G * kNacc] = fe;
+    __syncwarp();
+    for (int c = lane; c < kCols; c += 32) {
+      long long t = 0;
+      for (int l = 0; l < 32; l++)
+        t += red[w][l][c];
+      if (c == G * kNacc) {
+        wlj[w] = t;
+      } else if (p < a.ngroup) {
+        const int k = c / kNacc, comp = c % kNacc;
+        if (k < ns)
+          a.acc[(size_t) (si0 + k) * kAccStride + comp] = t;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+      for (int k = 0; k < G; k++)
+#pragma unroll
+        for (int c = 0; c < kNacc; c++)
+          fx[k][c] += __shfl_xor_sync(0xffffffffu, fx[k][c], off);
+      fe += __shfl_xor_sync(0xffffffffu, fe, off);
+    }
+    if (lane == 0)
+      wlj[w] = fe;
+    if (p < a.ngroup)
+#pragma unroll
+      for (int k = 0; k < G; k++)
+        if (lane == k && k < ns)
+#pragma unroll
+          for (int c = 0; c < kNacc; c++)
+            a.acc[(size_t) (si0 + k) * kAccStride + c] = fx[k][c];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long t = 0;
+    for (int k = 0; k < kMxWarps; k++)
+      t += wlj[k];
+    a.lj_part[blockIdx.x] = (double) t * kFxInv;
+  }
+}
+
+// ---- rigid-water fast path ------------------------------------------------------
+//
+// Every group is [O, H, H] with O carrying charge and LJ and the H sites
+// charge only (the site layout of ElecLJ's groups for 3-site water,
+// src/eleclj.cpp:654-676).  The nine site pairs and the one LJ pair of a
+// group pair are straight-line code; the partner's data is fetched while the
+// lane tests the anchor distance and parked in the shared-memory queue with
+// it, so the arithmetic phase reads only shared memory.  Per group pair the
+// kernel forms the FORCE on each row site (q E, plus LJ and switch terms on
+// O) and the pair energies, and converts those 11 values to fixed point.
+
+constexpr int kWaterQueue = 64;
+
+struct WaterArgs {
+  int ngroup, rowcap, geometric;
+  Box box;
+  double rhi2;
+  float rlo2, inv_sw, eta, c2, nel2;
+  const float4 *site;     // 3 slots per sorted group: offset from anchor, charge
+  const float2 *lj;       // per sorted group: anchor sigma, sqrt(epsilon)
+  const double4 *anchor;
+  const int *nbr, *nbr_count, *sorted, *group;
+  long long *acc;         // per site: slots 4..6 receive the force, 0..3 are cleared
+  double *lj_part, *ep_part;
+};
+
+__device__ __forceinline__ void water_site(float dx, float dy, float dz, float qbs, float eta, float nel2, float c2,
+                                           float &ex, float &ey, float &ez, float &ph, float &tq, float qb,
+                                           float &rinv_out)
+{
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  const float rinv = rsqrtf(r2);
+  float b0, b1;
+  ewald_f32(r2, rinv, eta, nel2, c2, b0, b1);
+  tq = fmaf(qb, b0, tq);
+  ph = fmaf(qbs, b0, ph);
+  const float f = qbs * b1;
+  ex = fmaf(f, dx, ex);
+  ey = fmaf(f, dy, ey);
+  ez = fmaf(f, dz, ez);
+  rinv_out = rinv;
+}
+
+__global__ void __launch_bounds__(kMxWarps * 32) k_pair_water(WaterArgs a)
+{
+  __shared__ float4 qa[kMxWarps][kWaterQueue];   // anchor displacement (xyz), anchor r^2
+  __shared__ float4 qo[kMxWarps][kWaterQueue];   // partner O: charge, sigma, sqrt(eps)
+  __shared__ float4 q1[kMxWarps][kWaterQueue];   // partner H1 offset, charge
+  __shared__ float4 q2[kMxWarps][kWaterQueue];   // partner H2 offset, charge
+  constexpr int kCols = 11;
+  __shared__ long long red[kMxWarps][32][kCols + 1];
+  __shared__ long long wsum[kMxWarps][2];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int p = blockIdx.x * kMxWarps + w;
+  long long fx[kCols];
+#pragma unroll
+  for (int c = 0; c < kCols; c++)
+    fx[c] = 0;
+  int si0 = 0;
+  if (p < a.ngroup) {
+    const float qO = a.site[3 * (size_t) p].w;
+    const float4 h1 = a.site[3 * (size_t) p + 1];
+    const float4 h2 = a.site[3 * (size_t) p + 2];
+    const float2 ljo = a.lj[p];
+    const double4 ai = a.anchor[p];
+    si0 = a.group[2 * a.sorted[p]];
+    const int cnt = a.nbr_count[p];
+    const int *row = a.nbr + (size_t) p * a.rowcap;
+    const unsigned below = (1u << lane) - 1;
+    int qn = 0;
+    auto compute = [&](int k) {
+      const float4 da = qa[w][k], jo = qo[w][k], j1 = q1[w][k], j2 = q2[w][k];
+      const float r2a = da.w;
+      float s = 1.f, ds = 0.f;
+      if (r2a > a.rlo2) {
+        const float z = (r2a - a.rlo2) * a.inv_sw;
+        s = fmaf(fmaf(fmaf(-6.f, z, 15.f), z, -10.f), z * z * z, 1.f);
+        ds = fmaf(fmaf(60.f, z, -120.f), z, 60.f) * z * z * a.inv_sw;
+      }
+      const float qbO = jo.x * s, qb1 = j1.w * s, qb2 = j2.w * s;
+      float eOx = 0.f, eOy = 0.f, eOz = 0.f, e1x = 0.f, e1y = 0.f, e1z = 0.f, e2x = 0.f, e2y = 0.f, e2z = 0.f;
+      float pO = 0.f, p1 = 0.f, p2 = 0.f, tO = 0.f, t1 = 0.f, t2 = 0.f, rOO, rtmp;
+      // row O (offset 0)
+      water_site(da.x, da.y, da.z, qbO, a.eta, a.nel2, a.c2, eOx, eOy, eOz, pO, tO, jo.x, rOO);
+      water_site(da.x - j1.x, da.y - j1.y, da.z - j1.z, qb1, a.eta, a.nel2, a.c2, eOx, eOy, eOz, pO, tO, j1.w, rtmp);
+      water_site(da.x - j2.x, da.y - j2.y, da.z - j2.z, qb2, a.eta, a.nel2, a.c2, eOx, eOy, eOz, pO, tO, j2.w, rtmp);
+      // row H1
+      const float c1x = da.x + h1.x, c1y = da.y + h1.y, c1z = da.z + h1.z;
+      water_site(c1x, c1y, c1z, qbO, a.eta, a.nel2, a.c2, e1x, e1y, e1z, p1, t1, jo.x, rtmp);
+      water_site(c1x - j1.x, c1y - j1.y, c1z - j1.z, qb1, a.eta, a.nel2, a.c2, e1x, e1y, e1z, p1, t1, j1.w, rtmp);
+      water_site(c1x - j2.x, c1y - j2.y, c1z - j2.z, qb2, a.eta, a.nel2, a.c2, e1x, e1y, e1z, p1, t1, j2.w, rtmp);
+      // row H2
+      const float c2x = da.x + h2.x, c2y = da.y + h2.y, c2z = da.z + h2.z;
+      water_site(c2x, c2y, c2z, qbO, a.eta, a.nel2, a.c2, e2x, e2y, e2z, p2, t2, jo.x, rtmp);
+      water_site(c2x - j1.x, c2y - j1.y, c2z - j1.z, qb1, a.eta, a.nel2, a.c2, e2x, e2y, e2z, p2, t2, j1.w, rtmp);
+      water_site(c2x - j2.x, c2y - j2.y, c2z - j2.z, qb2, a.eta, a.nel2, a.c2, e2x, e2y, e2z, p2, t2, j2.w, rtmp);
+      // O-O Lennard-Jones
+      const float sg = a.geometric ? ljo.x * jo.y : 0.5f * (ljo.x + jo.y);
+      const float s2 = a.geometric ? sg : sg * sg;
+      const float s6 = s2 * s2 * s2;
+      const float b = 4.f * ljo.y * jo.z * s6;
+      const float ir2 = rOO * rOO;
+      const float ir6 = ir2 * ir2 * ir2;
+      const float bi6 = b * ir6;
+      const float ai12 = b * s6 * ir6 * ir6;
+      const float u = ai12 - bi6;
+      const float du = (12.f * ai12 - 6.f * bi6) * ir2 * s;
+      // switch derivative on the anchors, scaled by the unswitched pair energy
+      const float g = ds * (qO * tO + h1.w * t1 + h2.w * t2 + u);
+      const float fo = du + g;
+      fx[0] += to_fx(fmaf(qO, eOx, fo * da.x));
+      fx[1] += to_fx(fmaf(qO, eOy, fo * da.y));
+      fx[2] += to_fx(fmaf(qO, eOz, fo * da.z));
+      fx[3] += to_fx(h1.w * e1x);
+      fx[4] += to_fx(h1.w * e1y);
+      fx[5] += to_fx(h1.w * e1z);
+      fx[6] += to_fx(h2.w * e2x);
+      fx[7] += to_fx(h2.w * e2y);
+      fx[8] += to_fx(h2.w * e2z);
+      fx[9] += to_fx(0.5f * fmaf(qO, pO, fmaf(h1.w, p1, h2.w * p2)));
+      fx[10] += to_fx(0.5f * u * s);
+    };
+    for (int base = 0; base < cnt; base += 32) {
+      const int e = base + lane;
+      bool take = false;
+      float4 da = make_float4(0.f, 0.f, 0.f, 0.f), jo = da, j1 = da, j2 = da;
+      if (e < cnt) {
+        const int q = row[e];
+        const double4 aj = a.anchor[q];
+        const float4 so = a.site[3 * (size_t) q];
+        j1 = a.site[3 * (size_t) q + 1];
+        j2 = a.site[3 * (size_t) q + 2];
+        const float2 lj = a.lj[q];
+        double x, y, z, sx, sy, sz;
+        const double r2a = anchor_disp(a.box, ai, aj, x, y, z, sx, sy, sz);
+        take = r2a <= a.rhi2;
+        da = make_float4((float) x, (float) y, (float) z, (float) r2a);
+        jo = make_float4(so.w, lj.x, lj.y, 0.f);
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, take);
+      if (take) {
+        const int idx = qn + __popc(bal & below);
+        qa[w][idx] = da;
+        qo[w][idx] = jo;
+        q1[w][idx] = j1;
+        q2[w][idx] = j2;
+      }
+      qn += __popc(bal);
+      __syncwarp();
+      if (qn >= 32) {
+        compute(lane);
+        __syncwarp();
+        if (lane < qn - 32) {
+          qa[w][lane] = qa[w][lane + 32];
+          qo[w][lane] = qo[w][lane + 32];
+          q1[w][lane] = q1[w][lane + 32];
+          q2[w][lane] = q2[w][lane + 32];
+        }
+        __syncwarp();
+        qn -= 32;
+      }
+    }
+    if (lane < qn)
+      compute(lane);
+  }
+#pragma unroll
+  for (int c = 0; c < kCols; c++)
+    red[w][lane][c] = fx[c];
+  __syncwarp();
+  if (lane < kCols) {
+    long long t = 0;
+    for (int l = 0; l < 32; l++)
+      t += red[w][l][lane];
+    if (lane < 9) {
+      if (p < a.ngroup)
+        a.acc[(size_t) (si0 + lane / 3) * kAccStride + 4 + lane % 3] = t;
+    } else {
+      wsum[w][lane - 9] = t;
+    }
+  } else if (lane < 11 + 12 && p < a.ngroup) {
+    // clear the potential and field slots of the three sites (P3M adds to them)
+    const int k = lane - 11;
+    a.acc[(size_t) (si0 + k / 4) * kAccStride + k % 4] = 0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long te = 0, tl = 0;
+    for (int k = 0; k < kMxWarps; k++) {
+      te += wsum[k][0];
+      tl += wsum[k][1];
+    }
+    a.ep_part[blockIdx.x] = (double) te * kFxInv;
+    a.lj_part[blockIdx.x] = (double) tl * kFxInv;
+  }
+}
+
+cudaError_t launch_rspace_water(mmnb_handle *h)
+{
+  WaterArgs a;
+  a.ngroup = h->ngroup;
+  a.rowcap = h->rowcap;
+  a.geometric = h->cfg.geometric_combining_for_sigma;
+  a.box = h->box;
+  a.rhi2 = h->rhi2;
+  a.rlo2 = (float) h->rlo2;
+  a.inv_sw = (float) h->inv_sw;
+  a.eta = (float) h->eta;
+  a.c2 = (float) (h->eta * M_2_SQRTPI);
+  a.nel2 = (float) (-h->eta * h->eta * M_LOG2E);
+  a.site = h->mx.site;
+  a.lj = h->mx.lj;
+  a.anchor = h->mx.anchor;
+  a.nbr = h->d_nbr;
+  a.nbr_count = h->d_nbr_count;
+  a.sorted = h->d_sorted;
+  a.group = h->d_group;
+  a.acc = h->mx.acc;
+  a.lj_part = h->d_lj_part;
+  a.ep_part = h->d_ep_part;
+  k_pair_water<<<pair_blocks(h), kMxWarps * 32, 0, h->stream>>>(a);
+  h->launches += 1;
+  return cudaGetLastError();
+}
+
+// Per step: sorted, padded FP32 slots (offset from anchor, charge, LJ
+// parameters, mask) and the FP64 anchors.
+__global__ void k_prep_mixed(const double *__restrict__ r, const double *__restrict__ q,
+                             const double *__restrict__ sig, const double *__restrict__ eps,
+                             const double *__restrict__ rscreen, const int *__restrict__ mask,
+                             const int *__restrict__ sorted, const int *__restrict__ group, int ngroup, int G,
+                             float4 *__restrict__ site, float4 *__restrict__ par, double4 *__restrict__ anchor,
+                             float2 *__restrict__ lj)
+{
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ngroup * G)
+    return;
+  const int p = s / G, k = s % G;
+  const int g = sorted[p];
+  const int a0 = group[2 * g];
+  const int st = a0 + k;
+  const double ax = r[3 * a0], ay = r[3 * a0 + 1], az = r[3 * a0 + 2];
+  if (k == 0) {
+    anchor[p] = make_double4(ax, ay, az, 0.0);
+    lj[p] = make_float2((float) sig[a0], (float) sqrt(eps[a0]));
+  }
+  if (st < group[2 * g + 1]) {
+    site[s] = make_float4((float) (r[3 * st] - ax), (float) (r[3 * st + 1] - ay), (float) (r[3 * st + 2] - az),
+                          (float) q[st]);
+    par[s] = make_float4((float) sig[st], (float) sqrt(eps[st]), (float) rscreen[st], __int_as_float(mask[st]));
+  } else {
+    site[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+    par[s] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
+  }
+}
+
+cudaError_t launch_prep_mixed(mmnb_handle *h, const double *d_r)
+{
+  const int n = h->ngroup * h->G;
+  k_prep_mixed<<<div_up(n, 256), 256, 0, h->stream>>>(d_r, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_mask,
+                                                      h->d_sorted, h->d_group, h->ngroup, h->G, h->mx.site,
+                                                      h->mx.par, h->mx.anchor, h->mx.lj);
+  h->launches += 1;
+  return cudaGetLastError();
+}
+
+template <int G, bool ANCHOR_LJ>
+static void launch_mixed_g(mmnb_handle *h, const MixedArgs &a)
+{
+  const int blocks = pair_blocks(h);
+  const int threads = kMxWarps * 32;
+  h->launches += 1;
+  if (h->has_rscreen) {
+    if (h->any_gexcl)
+      k_pair_mixed<G, true, true, ANCHOR_LJ><<<blocks, threads, 0, h->stream>>>(a);
+    else
+      k_pair_mixed<G, true, false, ANCHOR_LJ><<<blocks, threads, 0, h->stream>>>(a);
+  } else {
+    if (h->any_gexcl)
+      k_pair_mixed<G, false, true, ANCHOR_LJ><<<blocks, threads, 0, h->stream>>>(a);
+    else
+      k_pair_mixed<G, false, false, ANCHOR_LJ><<<blocks, threads, 0, h->stream>>>(a);
+  }
+}
+
+cudaError_t launch_rspace_mixed(mmnb_handle *h)
+{
+  MixedArgs a;
+  a.ngroup = h->ngroup;
+  a.rowcap = h->rowcap;
+  a.geometric = h->cfg.geometric_combining_for_sigma;
+  a.box = h->box;
+  a.rhi2 = h->rhi2;
+  a.rlo2 = (float) h->rlo2;
+  a.inv_sw = (float) h->inv_sw;
+  a.eta = (float) h->eta;
+  a.c2 = (float) (h->eta * M_2_SQRTPI);
+  a.nel2 = (float) (-h->eta * h->eta * M_LOG2E);
+  a.site = h->mx.site;
+  a.par = h->mx.par;
+  a.anchor = h->mx.anchor;
+  a.nbr = h->d_nbr;
+  a.nbr_count = h->d_nbr_count;
+  a.sorted = h->d_sorted;
+  a.group = h->d_group;
+  a.gexcl_ptr = h->d_gexcl_ptr;
+  a.gexcl_idx = h->d_gexcl_idx;
+  a.excl_ptr = h->d_excl_ptr;
+  a.excl_idx = h->d_excl_idx;
+  a.acc = h->mx.acc;
+  a.lj_part = h->d_lj_part;
+  const bool alj = h->lj_on_anchors_only;
+  switch (h->G) {
+  case 1: launch_mixed_g<1, false>(h, a); break;
+  case 2: alj ? launch_mixed_g<2, true>(h, a) : launch_mixed_g<2, false>(h, a); break;
+  case 3: alj ? launch_mixed_g<3, true>(h, a) : launch_mixed_g<3, false>(h, a); break;
+  case 4: alj ? launch_mixed_g<4, true>(h, a) : launch_mixed_g<4, false>(h, a); break;
+  default: launch_mixed_g<8, false>(h, a); break;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace mmnb

@@ -169,6 +169,11 @@ class ElecLJ:
         check(load().mmnb_get_counters(self._h, ctypes.byref(rb), ctypes.byref(ev)), self._h)
         return rb.value, ev.value
 
+    def launches(self):
+        n = ctypes.c_long()
+        check(load().mmnb_get_launches(self._h, ctypes.byref(n)), self._h)
+        return n.value
+
     def settings(self):
         rc, nlw, eta = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         mesh = np.zeros(3, dtype=np.int32)
