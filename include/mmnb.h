@@ -199,6 +199,25 @@ int mmnb_chebyshev_table(double rc, double eta, double *min, double *max,
    429-431). */
 int mmnb_p3m_mesh_size(double a, double grid_spacing);
 
+/* Ordinary Ewald reciprocal-space potential and field, ADDED to d_phi (nsite)
+   and d_evec (3*nsite), for callers that cannot allocate device memory — a
+   host that has reserved all device memory for its own pool, or a loop that
+   must not let an allocation or free synchronise the device.  It allocates
+   nothing: positions d_r (3*nsite), charges d_q and both outputs are the
+   caller's device arrays, and the only scratch is a fixed array inside the
+   library, one per device for the life of the process, holding at most 4096
+   wave vectors (|n| <= about 12); a larger kspace_cutoff returns MMNB_ERR_ARG
+   with an explanation in mmnb_last_error(NULL).  The first call on a device
+   looks up that array's device address; make that first call before any
+   stream capture.  All calls on a device share the array and overwrite it, so
+   calls that overlap on the GPU race.  bctype MMNB_CUBIC (box[0]) or
+   MMNB_ORTHORHOMBIC; stream is a cudaStream_t or NULL.  The launches are
+   asynchronous on that stream.  This entry point has no counterpart in the
+   reference: it is the computation of kspace_field without kspace_new. */
+int mmnb_kspace_field_noalloc(int nsite, const double *d_r, const double *d_q, int bctype,
+                              const double box[3], double eta, double kspace_cutoff,
+                              double *d_phi, double *d_evec, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

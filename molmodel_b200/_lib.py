@@ -77,6 +77,8 @@ SIGNATURES = [
     ("mmnb_status_string", ctypes.c_char_p, [ctypes.c_int]),
     ("mmnb_chebyshev_table", ctypes.c_int, [ctypes.c_double, ctypes.c_double, _dp, _dp, _dp, _dp]),
     ("mmnb_p3m_mesh_size", ctypes.c_int, [ctypes.c_double, ctypes.c_double]),
+    ("mmnb_kspace_field_noalloc", ctypes.c_int, [ctypes.c_int, _vp, _vp, ctypes.c_int, _dp, ctypes.c_double,
+                                                 ctypes.c_double, _vp, _vp, _vp]),
 ]
 
 _lib = None

@@ -401,6 +401,12 @@ void free_all(mmnb_handle *h)
 
 namespace mmnb {
 
+int set_global_error(int code, const std::string &msg)
+{
+  g_create_error = msg;
+  return code;
+}
+
 void timing_mark(mmnb_handle *h, const char *name)
 {
   Timing &t = h->timing;

@@ -201,6 +201,7 @@ cudaError_t launch_energy(mmnb_handle *h, double *d_energy);
 
 // helpers shared by the .cu files
 void timing_mark(mmnb_handle *h, const char *name);
+int set_global_error(int code, const std::string &msg);  // read back by mmnb_last_error(NULL)
 int pair_blocks(const mmnb_handle *h);
 int excl_blocks(const mmnb_handle *h);
 
