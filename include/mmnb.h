@@ -147,6 +147,16 @@ int mmnb_compute(mmnb_handle *h, const double *r, double *f, double *u,
    once the handle has done one mmnb_compute (first-call set-up). */
 int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *d_energy);
 
+/* Capture one mmnb_compute_device(h, d_r, d_f, d_energy) into a CUDA graph on
+   the handle's stream (which must be a non-default stream, see
+   mmnb_set_stream); mmnb_graph_launch replays it.  The graph reads d_r and
+   writes d_f / d_energy at the addresses given here, and it keeps the
+   device-side rebuild test, so replaying it is exactly one more evaluation.
+   Call after the handle's first evaluation; capture again after mmnb_scale,
+   mmnb_set_params or anything that reallocates (a neighbour-row overflow). */
+int mmnb_graph_capture(mmnb_handle *h, const double *d_r, double *d_f, double *d_energy);
+int mmnb_graph_launch(mmnb_handle *h);
+
 /* Volume move by factor s: box, eta /= s, Chebyshev table, influence function
    and cell stencil follow (src/eleclj.cpp:1268-1280, src/pppm.c:643-664). */
 int mmnb_scale(mmnb_handle *h, double s);

@@ -63,6 +63,8 @@ SIGNATURES = [
     ("mmnb_set_params", ctypes.c_int, [_vp, _ip, _dp, _dp, _dp, _dp]),
     ("mmnb_compute", ctypes.c_int, [_vp, _dp, _dp, _dp, ctypes.POINTER(MmnbEnergy), _dp, _dp]),
     ("mmnb_compute_device", ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    ("mmnb_graph_capture", ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    ("mmnb_graph_launch", ctypes.c_int, [_vp]),
     ("mmnb_scale", ctypes.c_int, [_vp, ctypes.c_double]),
     ("mmnb_set_stream", ctypes.c_int, [_vp, _vp]),
     ("mmnb_get_pairlist", ctypes.c_int, [_vp, _lp, _ip, ctypes.c_long]),

@@ -395,6 +395,10 @@ void free_all(mmnb_handle *h)
     cufftDestroy(h->plan_c2r32);
   for (auto e : h->timing.pool)
     cudaEventDestroy(e);
+  if (h->graph_exec)
+    cudaGraphExecDestroy(h->graph_exec);
+  if (h->graph)
+    cudaGraphDestroy(h->graph);
 }
 
 }  // namespace
@@ -410,7 +414,7 @@ int set_global_error(int code, const std::string &msg)
 void timing_mark(mmnb_handle *h, const char *name)
 {
   Timing &t = h->timing;
-  if (!t.on)
+  if (!t.on || h->capturing)
     return;
   if (t.used == t.pool.size()) {
     cudaEvent_t e;
@@ -799,6 +803,52 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
   h->first = false;
   h->force_rebuild_next = 0;
   h->evals++;
+  return MMNB_OK;
+}
+
+int mmnb_graph_capture(mmnb_handle *h, const double *d_r, double *d_f, double *d_energy)
+{
+  if (!h || !d_r)
+    return fail(h, MMNB_ERR_ARG, "null handle or positions");
+  if (h->first)
+    return fail(h, MMNB_ERR_STATE, "evaluate once (mmnb_compute) before capturing");
+  if (h->stream == nullptr)
+    return fail(h, MMNB_ERR_STATE, "capture needs a non-default stream");
+  if (h->graph_exec) {
+    cudaGraphExecDestroy(h->graph_exec);
+    h->graph_exec = nullptr;
+  }
+  if (h->graph) {
+    cudaGraphDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  h->capturing = true;
+  const long ev = h->evals, ln = h->launches;
+  const int s = mmnb_compute_device(h, d_r, d_f, d_energy);
+  h->capturing = false;
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+  h->evals = ev;
+  h->launch_per_eval = h->launches - ln;
+  h->launches = ln;
+  if (s)
+    return s;
+  if (e != cudaSuccess)
+    return fail(h, MMNB_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+  h->graph = g;
+  CK(cudaGraphInstantiate(&h->graph_exec, h->graph, 0));
+  return MMNB_OK;
+}
+
+int mmnb_graph_launch(mmnb_handle *h)
+{
+  if (!h || !h->graph_exec)
+    return fail(h, MMNB_ERR_STATE, "no captured evaluation");
+  CK(cudaGraphLaunch(h->graph_exec, h->stream));
+  h->evals++;
+  h->launches += h->launch_per_eval;
   return MMNB_OK;
 }
 

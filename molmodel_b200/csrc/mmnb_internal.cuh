@@ -127,6 +127,7 @@ struct mmnb_handle {
   int *h_flags = nullptr;            // pinned mirror
   long rebuilds = 0, evals = 0;
   long launches = 0;                 // kernels of this library launched so far
+  long launch_per_eval = 0;          // kernels in the captured evaluation
   bool first = true;
   int force_rebuild_next = 0;
 
@@ -177,6 +178,11 @@ struct mmnb_handle {
   mmnb::MixedBufs mx;
 
   mmnb::Timing timing;
+
+  // one captured evaluation (mmnb_graph_capture / mmnb_graph_launch)
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  bool capturing = false;
 };
 
 namespace mmnb {

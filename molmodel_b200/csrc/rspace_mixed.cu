@@ -8,9 +8,10 @@
 //     site-pair displacement is (anchor displacement, FP64 -> FP32) plus the
 //     difference of two small offsets: relative precision ~1e-7 at any box
 //     size, although the unwrapped coordinates themselves can be large;
-//   * erfc(eta r) uses Abramowitz & Stegun 7.1.26 (Hastings' rational
-//     approximation, |error| <= 1.5e-7), with exp(-eta^2 r^2) shared with the
-//     field term b1 = (b0 + 2 eta/sqrt(pi) exp(-eta^2 r^2)) / r^2;
+//   * erfc(eta r) = t P(t) exp(-eta^2 r^2) with t = 1/(1 + p eta r): the
+//     form of Hastings' approximation with a degree-7 P refitted for
+//     relative accuracy (below), exp(-eta^2 r^2) shared with the field term
+//     b1 = (b0 + 2 eta/sqrt(pi) exp(-eta^2 r^2)) / r^2;
 //   * the switch and LJ terms are the FP64 form's formulas in FP32.
 // Each group pair's contribution to each row site (potential, field, LJ
 // force) is summed in FP32 and then converted to 64-bit fixed point
@@ -355,7 +356,7 @@ __device__ __forceinline__ void water_site(float dx, float dy, float dz, float q
   rinv_out = rinv;
 }
 
-__global__ void __launch_bounds__(kMxWarps * 32) k_pair_water(WaterArgs a)
+__global__ void __launch_bounds__(kMxWarps * 32, 5) k_pair_water(WaterArgs a)
 {
   __shared__ float4 qa[kMxWarps][kWaterQueue];   // anchor displacement (xyz), anchor r^2
   __shared__ float4 qo[kMxWarps][kWaterQueue];   // partner O: charge, sigma, sqrt(eps)
@@ -434,23 +435,52 @@ __global__ void __launch_bounds__(kMxWarps * 32) k_pair_water(WaterArgs a)
       fx[9] += to_fx(0.5f * fmaf(qO, pO, fmaf(h1.w, p1, h2.w * p2)));
       fx[10] += to_fx(0.5f * u * s);
     };
+    // partner data of the current batch of 32 list entries
+    int qc = lane < cnt ? row[lane] : -1;
+    double4 aj_c = make_double4(0, 0, 0, 0);
+    float4 so_c = make_float4(0.f, 0.f, 0.f, 0.f), j1_c = so_c, j2_c = so_c;
+    float2 lj_c = make_float2(0.f, 0.f);
+    if (qc >= 0) {
+      aj_c = a.anchor[qc];
+      so_c = a.site[3 * (size_t) qc];
+      j1_c = a.site[3 * (size_t) qc + 1];
+      j2_c = a.site[3 * (size_t) qc + 2];
+      lj_c = a.lj[qc];
+    }
     for (int base = 0; base < cnt; base += 32) {
       const int e = base + lane;
       bool take = false;
-      float4 da = make_float4(0.f, 0.f, 0.f, 0.f), jo = da, j1 = da, j2 = da;
-      if (e < cnt) {
-        const int q = row[e];
-        const double4 aj = a.anchor[q];
-        const float4 so = a.site[3 * (size_t) q];
-        j1 = a.site[3 * (size_t) q + 1];
-        j2 = a.site[3 * (size_t) q + 2];
-        const float2 lj = a.lj[q];
-        double x, y, z, sx, sy, sz;
-        const double r2a = anchor_disp(a.box, ai, aj, x, y, z, sx, sy, sz);
-        take = r2a <= a.rhi2;
-        da = make_float4((float) x, (float) y, (float) z, (float) r2a);
-        jo = make_float4(so.w, lj.x, lj.y, 0.f);
+      // request the next batch's partner data now, so its latency overlaps
+      // this batch's distance tests and arithmetic
+      const int en = e + 32;
+      const int qnx = en < cnt ? row[en] : -1;
+      double4 aj_n = make_double4(0, 0, 0, 0);
+      float4 so_n = make_float4(0.f, 0.f, 0.f, 0.f), j1_n = so_n, j2_n = so_n;
+      float2 lj_n = make_float2(0.f, 0.f);
+      if (qnx >= 0) {
+        aj_n = a.anchor[qnx];
+        so_n = a.site[3 * (size_t) qnx];
+        j1_n = a.site[3 * (size_t) qnx + 1];
+        j2_n = a.site[3 * (size_t) qnx + 2];
+        lj_n = a.lj[qnx];
       }
+      float4 da = make_float4(0.f, 0.f, 0.f, 0.f), jo = da;
+      if (qc >= 0) {
+        double x, y, z, sx, sy, sz;
+        const double r2a = anchor_disp(a.box, ai, aj_c, x, y, z, sx, sy, sz);
+        take = r2a <= a.rhi2;
+        if (take) {
+          da = make_float4((float) x, (float) y, (float) z, (float) r2a);
+          jo = make_float4(so_c.w, lj_c.x, lj_c.y, 0.f);
+        }
+      }
+      const float4 j1 = j1_c, j2 = j2_c;
+      qc = qnx;
+      aj_c = aj_n;
+      so_c = so_n;
+      j1_c = j1_n;
+      j2_c = j2_n;
+      lj_c = lj_n;
       const unsigned bal = __ballot_sync(0xffffffffu, take);
       if (take) {
         const int idx = qn + __popc(bal & below);
@@ -546,24 +576,25 @@ __global__ void k_prep_mixed(const double *__restrict__ r, const double *__restr
                              float2 *__restrict__ lj)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= ngroup * G)
-    return;
-  const int p = s / G, k = s % G;
-  const int g = sorted[p];
-  const int a0 = group[2 * g];
-  const int st = a0 + k;
-  const double ax = r[3 * a0], ay = r[3 * a0 + 1], az = r[3 * a0 + 2];
-  if (k == 0) {
-    anchor[p] = make_double4(ax, ay, az, 0.0);
-    lj[p] = make_float2((float) sig[a0], (float) sqrt(eps[a0]));
-  }
-  if (st < group[2 * g + 1]) {
-    site[s] = make_float4((float) (r[3 * st] - ax), (float) (r[3 * st + 1] - ay), (float) (r[3 * st + 2] - az),
-                          (float) q[st]);
-    par[s] = make_float4((float) sig[st], (float) sqrt(eps[st]), (float) rscreen[st], __int_as_float(mask[st]));
-  } else {
-    site[s] = make_float4(0.f, 0.f, 0.f, 0.f);
-    par[s] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
+  if (s < ngroup * G) {
+    const int p = s / G, k = s % G;
+    const int g = sorted[p];
+    const int a0 = group[2 * g];
+    const int st = a0 + k;
+    const double ax = r[3 * a0], ay = r[3 * a0 + 1], az = r[3 * a0 + 2];
+    if (k == 0) {
+      anchor[p] = make_double4(ax, ay, az, 0.0);
+      lj[p] = make_float2((float) sig[a0], (float) sqrt(eps[a0]));
+    }
+    if (st < group[2 * g + 1]) {
+      const float ox = (float) (r[3 * st] - ax), oy = (float) (r[3 * st + 1] - ay),
+                  oz = (float) (r[3 * st + 2] - az);
+      site[s] = make_float4(ox, oy, oz, (float) q[st]);
+      par[s] = make_float4((float) sig[st], (float) sqrt(eps[st]), (float) rscreen[st], __int_as_float(mask[st]));
+    } else {
+      site[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+      par[s] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
+    }
   }
 }
 

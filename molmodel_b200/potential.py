@@ -142,6 +142,14 @@ class ElecLJ:
         check(load().mmnb_compute_device(self._h, ctypes.c_void_p(d_r), ctypes.c_void_p(d_f),
                                          ctypes.c_void_p(d_energy)), self._h)
 
+    def graph_capture(self, d_r, d_f, d_energy):
+        """Capture one device evaluation into a CUDA graph (mmnb_graph_capture)."""
+        check(load().mmnb_graph_capture(self._h, ctypes.c_void_p(d_r), ctypes.c_void_p(d_f),
+                                        ctypes.c_void_p(d_energy)), self._h)
+
+    def graph_launch(self):
+        check(load().mmnb_graph_launch(self._h), self._h)
+
     def set_stream(self, stream_ptr):
         check(load().mmnb_set_stream(self._h, ctypes.c_void_p(stream_ptr)), self._h)
 
