@@ -46,6 +46,15 @@ __device__ __forceinline__ float ex2_approx(float x)
   return y;
 }
 
+// r^2 of two distinct sites is a normal number, so the flush-to-zero form
+// (no denormal fix-up around the MUFU op) gives rsqrtf's result
+__device__ __forceinline__ float rsqrt_approx(float x)
+{
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 __device__ __forceinline__ float rcp_approx(float x)
 {
   float y;
@@ -133,7 +142,7 @@ __device__ __forceinline__ void pair_mixed(const MixedArgs &a, const float4 (&oi
         continue;
       const float dx = cx - oj[jb].x, dy = cy - oj[jb].y, dz = cz - oj[jb].z;
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      const float rinv = rsqrtf(r2);
+      const float rinv = rsqrt_approx(r2);
       if (m & MMNB_SITE_HAS_Q) {
         float b0, b1;
         ewald_f32(r2, rinv, a.eta, a.nel2, a.c2, b0, b1);
@@ -318,19 +327,24 @@ __global__ void __launch_bounds__(kMxWarps * 32) k_pair_mixed(MixedArgs a)
 // Every group is [O, H, H] with O carrying charge and LJ and the H sites
 // charge only (the site layout of ElecLJ's groups for 3-site water,
 // src/eleclj.cpp:654-676).  The nine site pairs and the one LJ pair of a
-// group pair are straight-line code; the partner's data is fetched while the
-// lane tests the anchor distance and parked in the shared-memory queue with
-// it, so the arithmetic phase reads only shared memory.  Per group pair the
-// kernel forms the FORCE on each row site (q E, plus LJ and switch terms on
-// O) and the pair energies, and converts those 11 values to fixed point.
+// group pair are straight-line code.  A warp owns one row group and walks its
+// list 32 entries at a time: each lane tests one partner's FP64 anchor
+// distance (anchors are requested one batch ahead, list indices two batches
+// ahead), and for an accepted partner writes the FP32 anchor displacement to
+// a 64-slot shared-memory ring and starts asynchronous copies (cp.async) of
+// the partner's three site slots and LJ parameters into the same ring slot.
+// When 32 entries are queued every lane evaluates one group pair from shared
+// memory.  Per group pair the kernel forms the FORCE on each row site (q E,
+// plus LJ and switch terms on O) and the pair energies, and converts those 11
+// values to fixed point.
 
-constexpr int kWaterQueue = 64;
+constexpr int kWaterRing = 128;
 
 struct WaterArgs {
   int ngroup, rowcap, geometric;
   Box box;
   double rhi2;
-  float rlo2, inv_sw, eta, c2, nel2;
+  float rlo2, inv_sw, pe, c2, nel2;  // pe = p eta (erfc argument scale)
   const float4 *site;     // 3 slots per sorted group: offset from anchor, charge
   const float2 *lj;       // per sorted group: anchor sigma, sqrt(epsilon)
   const double4 *anchor;
@@ -339,38 +353,66 @@ struct WaterArgs {
   double *lj_part, *ep_part;
 };
 
-__device__ __forceinline__ void water_site(float dx, float dy, float dz, float qbs, float eta, float nel2, float c2,
-                                           float &ex, float &ey, float &ez, float &ph, float &tq, float qb,
-                                           float &rinv_out)
+// One site pair of a water group pair: adds q_j b1 S d to the row site's field
+// sum (qbs = q_j S) and q_j b0 to its unswitched potential sum (qb = q_j).
+// b0 = erfc(eta r)/r, b1 = (b0 + c2 exp(-eta^2 r^2))/r^2.
+__device__ __forceinline__ void water_site(float dx, float dy, float dz, float qb, float qbs, const WaterArgs &a,
+                                           float &ex, float &ey, float &ez, float &tq, float &rinv_out)
 {
   const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  const float rinv = rsqrtf(r2);
-  float b0, b1;
-  ewald_f32(r2, rinv, eta, nel2, c2, b0, b1);
+  const float rinv = rsqrt_approx(r2);
+  const float t = rcp_approx(fmaf(a.pe, r2 * rinv, 1.f));
+  float p = fmaf(kE7, t, kE6);
+  p = fmaf(p, t, kE5);
+  p = fmaf(p, t, kE4);
+  p = fmaf(p, t, kE3);
+  p = fmaf(p, t, kE2);
+  p = fmaf(p, t, kE1);
+  p = fmaf(p, t, kE0);
+  const float e = ex2_approx(r2 * a.nel2);
+  const float b0 = (t * p) * (e * rinv);
   tq = fmaf(qb, b0, tq);
-  ph = fmaf(qbs, b0, ph);
-  const float f = qbs * b1;
+  const float f = fmaf(a.c2, e, b0) * (rinv * rinv) * qbs;
   ex = fmaf(f, dx, ex);
   ey = fmaf(f, dy, ey);
   ez = fmaf(f, dz, ez);
   rinv_out = rinv;
 }
 
-__global__ void __launch_bounds__(kMxWarps * 32, 5) k_pair_water(WaterArgs a)
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
 {
-  __shared__ float4 qa[kMxWarps][kWaterQueue];   // anchor displacement (xyz), anchor r^2
-  __shared__ float4 qo[kMxWarps][kWaterQueue];   // partner O: charge, sigma, sqrt(eps)
-  __shared__ float4 q1[kMxWarps][kWaterQueue];   // partner H1 offset, charge
-  __shared__ float4 q2[kMxWarps][kWaterQueue];   // partner H2 offset, charge
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"((unsigned) __cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+
+__device__ __forceinline__ void cp_async8(void *dst, const void *src)
+{
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned) __cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+__global__ void __launch_bounds__(kMxWarps * 32, 4) k_pair_water(WaterArgs a)
+{
+  // per warp: ring of anchor displacement (xyz, r^2), partner O slot (zero
+  // offset, charge), H1 and H2 slots (offset, charge); LJ parameters apart
+  __shared__ float4 ring[kMxWarps][4][kWaterRing];
+  __shared__ float2 ql[kMxWarps][kWaterRing];   // partner sigma, sqrt(eps)
   constexpr int kCols = 11;
-  __shared__ long long red[kMxWarps][32][kCols + 1];
-  __shared__ long long wsum[kMxWarps][2];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int p = blockIdx.x * kMxWarps + w;
+  constexpr int kMask = kWaterRing - 1;
+  constexpr float kTwo32 = 4294967296.0f, kTwo31 = 2147483648.0f;
   long long fx[kCols];
 #pragma unroll
   for (int c = 0; c < kCols; c++)
     fx[c] = 0;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int p = blockIdx.x * kMxWarps + w;
+  float4 *qa = ring[w][0], *q0 = ring[w][1], *q1 = ring[w][2], *q2 = ring[w][3];
   int si0 = 0;
   if (p < a.ngroup) {
     const float qO = a.site[3 * (size_t) p].w;
@@ -378,13 +420,17 @@ __global__ void __launch_bounds__(kMxWarps * 32, 5) k_pair_water(WaterArgs a)
     const float4 h2 = a.site[3 * (size_t) p + 2];
     const float2 ljo = a.lj[p];
     const double4 ai = a.anchor[p];
+    // charges times the fixed-point scale: the converted values come out of
+    // the last product directly
+    const float qO32 = qO * kTwo32, qH1_32 = h1.w * kTwo32, qH2_32 = h2.w * kTwo32;
     si0 = a.group[2 * a.sorted[p]];
     const int cnt = a.nbr_count[p];
     const int *row = a.nbr + (size_t) p * a.rowcap;
     const unsigned below = (1u << lane) - 1;
-    int qn = 0;
     auto compute = [&](int k) {
-      const float4 da = qa[w][k], jo = qo[w][k], j1 = q1[w][k], j2 = q2[w][k];
+      const float4 da = qa[k], j1 = q1[k], j2 = q2[k];
+      const float qj = q0[k].w;
+      const float2 lj = ql[w][k];
       const float r2a = da.w;
       float s = 1.f, ds = 0.f;
       if (r2a > a.rlo2) {
@@ -392,129 +438,111 @@ __global__ void __launch_bounds__(kMxWarps * 32, 5) k_pair_water(WaterArgs a)
         s = fmaf(fmaf(fmaf(-6.f, z, 15.f), z, -10.f), z * z * z, 1.f);
         ds = fmaf(fmaf(60.f, z, -120.f), z, 60.f) * z * z * a.inv_sw;
       }
-      const float qbO = jo.x * s, qb1 = j1.w * s, qb2 = j2.w * s;
+      const float qbO = qj * s, qb1 = j1.w * s, qb2 = j2.w * s;
       float eOx = 0.f, eOy = 0.f, eOz = 0.f, e1x = 0.f, e1y = 0.f, e1z = 0.f, e2x = 0.f, e2y = 0.f, e2z = 0.f;
-      float pO = 0.f, p1 = 0.f, p2 = 0.f, tO = 0.f, t1 = 0.f, t2 = 0.f, rOO, rtmp;
+      float tO = 0.f, t1 = 0.f, t2 = 0.f, rOO, rtmp;
       // row O (offset 0)
-      water_site(da.x, da.y, da.z, qbO, a.eta, a.nel2, a.c2, eOx, eOy, eOz, pO, tO, jo.x, rOO);
-      water_site(da.x - j1.x, da.y - j1.y, da.z - j1.z, qb1, a.eta, a.nel2, a.c2, eOx, eOy, eOz, pO, tO, j1.w, rtmp);
-      water_site(da.x - j2.x, da.y - j2.y, da.z - j2.z, qb2, a.eta, a.nel2, a.c2, eOx, eOy, eOz, pO, tO, j2.w, rtmp);
+      water_site(da.x, da.y, da.z, qj, qbO, a, eOx, eOy, eOz, tO, rOO);
+      water_site(da.x - j1.x, da.y - j1.y, da.z - j1.z, j1.w, qb1, a, eOx, eOy, eOz, tO, rtmp);
+      water_site(da.x - j2.x, da.y - j2.y, da.z - j2.z, j2.w, qb2, a, eOx, eOy, eOz, tO, rtmp);
       // row H1
       const float c1x = da.x + h1.x, c1y = da.y + h1.y, c1z = da.z + h1.z;
-      water_site(c1x, c1y, c1z, qbO, a.eta, a.nel2, a.c2, e1x, e1y, e1z, p1, t1, jo.x, rtmp);
-      water_site(c1x - j1.x, c1y - j1.y, c1z - j1.z, qb1, a.eta, a.nel2, a.c2, e1x, e1y, e1z, p1, t1, j1.w, rtmp);
-      water_site(c1x - j2.x, c1y - j2.y, c1z - j2.z, qb2, a.eta, a.nel2, a.c2, e1x, e1y, e1z, p1, t1, j2.w, rtmp);
+      water_site(c1x, c1y, c1z, qj, qbO, a, e1x, e1y, e1z, t1, rtmp);
+      water_site(c1x - j1.x, c1y - j1.y, c1z - j1.z, j1.w, qb1, a, e1x, e1y, e1z, t1, rtmp);
+      water_site(c1x - j2.x, c1y - j2.y, c1z - j2.z, j2.w, qb2, a, e1x, e1y, e1z, t1, rtmp);
       // row H2
       const float c2x = da.x + h2.x, c2y = da.y + h2.y, c2z = da.z + h2.z;
-      water_site(c2x, c2y, c2z, qbO, a.eta, a.nel2, a.c2, e2x, e2y, e2z, p2, t2, jo.x, rtmp);
-      water_site(c2x - j1.x, c2y - j1.y, c2z - j1.z, qb1, a.eta, a.nel2, a.c2, e2x, e2y, e2z, p2, t2, j1.w, rtmp);
-      water_site(c2x - j2.x, c2y - j2.y, c2z - j2.z, qb2, a.eta, a.nel2, a.c2, e2x, e2y, e2z, p2, t2, j2.w, rtmp);
+      water_site(c2x, c2y, c2z, qj, qbO, a, e2x, e2y, e2z, t2, rtmp);
+      water_site(c2x - j1.x, c2y - j1.y, c2z - j1.z, j1.w, qb1, a, e2x, e2y, e2z, t2, rtmp);
+      water_site(c2x - j2.x, c2y - j2.y, c2z - j2.z, j2.w, qb2, a, e2x, e2y, e2z, t2, rtmp);
       // O-O Lennard-Jones
-      const float sg = a.geometric ? ljo.x * jo.y : 0.5f * (ljo.x + jo.y);
+      const float sg = a.geometric ? ljo.x * lj.x : 0.5f * (ljo.x + lj.x);
       const float s2 = a.geometric ? sg : sg * sg;
       const float s6 = s2 * s2 * s2;
-      const float b = 4.f * ljo.y * jo.z * s6;
+      const float b = 4.f * ljo.y * lj.y * s6;
       const float ir2 = rOO * rOO;
       const float ir6 = ir2 * ir2 * ir2;
       const float bi6 = b * ir6;
       const float ai12 = b * s6 * ir6 * ir6;
       const float u = ai12 - bi6;
       const float du = (12.f * ai12 - 6.f * bi6) * ir2 * s;
-      // switch derivative on the anchors, scaled by the unswitched pair energy
-      const float g = ds * (qO * tO + h1.w * t1 + h2.w * t2 + u);
-      const float fo = du + g;
-      fx[0] += to_fx(fmaf(qO, eOx, fo * da.x));
-      fx[1] += to_fx(fmaf(qO, eOy, fo * da.y));
-      fx[2] += to_fx(fmaf(qO, eOz, fo * da.z));
-      fx[3] += to_fx(h1.w * e1x);
-      fx[4] += to_fx(h1.w * e1y);
-      fx[5] += to_fx(h1.w * e1z);
-      fx[6] += to_fx(h2.w * e2x);
-      fx[7] += to_fx(h2.w * e2y);
-      fx[8] += to_fx(h2.w * e2z);
-      fx[9] += to_fx(0.5f * fmaf(qO, pO, fmaf(h1.w, p1, h2.w * p2)));
-      fx[10] += to_fx(0.5f * u * s);
+      // unswitched Coulomb energy of the group pair; its switched half is the
+      // row's energy share and, with u, it scales the switch derivative
+      const float tq = fmaf(qO, tO, fmaf(h1.w, t1, h2.w * t2));
+      const float g = ds * (tq + u);
+      const float fo32 = (du + g) * kTwo32;
+      const float s31 = s * kTwo31;
+      fx[0] += __float2ll_rn(fmaf(qO32, eOx, fo32 * da.x));
+      fx[1] += __float2ll_rn(fmaf(qO32, eOy, fo32 * da.y));
+      fx[2] += __float2ll_rn(fmaf(qO32, eOz, fo32 * da.z));
+      fx[3] += __float2ll_rn(qH1_32 * e1x);
+      fx[4] += __float2ll_rn(qH1_32 * e1y);
+      fx[5] += __float2ll_rn(qH1_32 * e1z);
+      fx[6] += __float2ll_rn(qH2_32 * e2x);
+      fx[7] += __float2ll_rn(qH2_32 * e2y);
+      fx[8] += __float2ll_rn(qH2_32 * e2z);
+      fx[9] += __float2ll_rn(tq * s31);
+      fx[10] += __float2ll_rn(u * s31);
     };
-    // partner data of the current batch of 32 list entries
-    int qc = lane < cnt ? row[lane] : -1;
-    double4 aj_c = make_double4(0, 0, 0, 0);
-    float4 so_c = make_float4(0.f, 0.f, 0.f, 0.f), j1_c = so_c, j2_c = so_c;
-    float2 lj_c = make_float2(0.f, 0.f);
-    if (qc >= 0) {
-      aj_c = a.anchor[qc];
-      so_c = a.site[3 * (size_t) qc];
-      j1_c = a.site[3 * (size_t) qc + 1];
-      j2_c = a.site[3 * (size_t) qc + 2];
-      lj_c = a.lj[qc];
-    }
+    // Entries past the row end read the row's own group (a valid address);
+    // they are never accepted.
+    int jc = lane < cnt ? row[lane] : p;
+    int jn = lane + 32 < cnt ? row[lane + 32] : p;
+    double4 ac = a.anchor[jc];
+    int head = 0, qn = 0;  // ring entries [head, head + qn)
     for (int base = 0; base < cnt; base += 32) {
-      const int e = base + lane;
-      bool take = false;
-      // request the next batch's partner data now, so its latency overlaps
-      // this batch's distance tests and arithmetic
-      const int en = e + 32;
-      const int qnx = en < cnt ? row[en] : -1;
-      double4 aj_n = make_double4(0, 0, 0, 0);
-      float4 so_n = make_float4(0.f, 0.f, 0.f, 0.f), j1_n = so_n, j2_n = so_n;
-      float2 lj_n = make_float2(0.f, 0.f);
-      if (qnx >= 0) {
-        aj_n = a.anchor[qnx];
-        so_n = a.site[3 * (size_t) qnx];
-        j1_n = a.site[3 * (size_t) qnx + 1];
-        j2_n = a.site[3 * (size_t) qnx + 2];
-        lj_n = a.lj[qnx];
-      }
-      float4 da = make_float4(0.f, 0.f, 0.f, 0.f), jo = da;
-      if (qc >= 0) {
-        double x, y, z, sx, sy, sz;
-        const double r2a = anchor_disp(a.box, ai, aj_c, x, y, z, sx, sy, sz);
-        take = r2a <= a.rhi2;
-        if (take) {
-          da = make_float4((float) x, (float) y, (float) z, (float) r2a);
-          jo = make_float4(so_c.w, lj_c.x, lj_c.y, 0.f);
-        }
-      }
-      const float4 j1 = j1_c, j2 = j2_c;
-      qc = qnx;
-      aj_c = aj_n;
-      so_c = so_n;
-      j1_c = j1_n;
-      j2_c = j2_n;
-      lj_c = lj_n;
+      const int e2 = base + 64 + lane;
+      const int jnn = e2 < cnt ? row[e2] : p;
+      const double4 an = a.anchor[jn];
+      double x, y, z, sx, sy, sz;
+      const double r2a = anchor_disp(a.box, ai, ac, x, y, z, sx, sy, sz);
+      const bool take = base + lane < cnt && r2a <= a.rhi2;
       const unsigned bal = __ballot_sync(0xffffffffu, take);
       if (take) {
-        const int idx = qn + __popc(bal & below);
-        qa[w][idx] = da;
-        qo[w][idx] = jo;
-        q1[w][idx] = j1;
-        q2[w][idx] = j2;
+        const int slot = (head + qn + __popc(bal & below)) & kMask;
+        qa[slot] = make_float4((float) x, (float) y, (float) z, (float) r2a);
+        const float4 *src = a.site + 3 * (size_t) jc;
+        cp_async16(&q0[slot], src);
+        cp_async16(&q1[slot], src + 1);
+        cp_async16(&q2[slot], src + 2);
+        cp_async8(&ql[w][slot], a.lj + jc);
       }
+      cp_async_commit();
+      // entries of earlier batches are evaluated one batch after their copies
+      // were started, so the copies are normally complete by then
+      const bool run = qn >= 32;
       qn += __popc(bal);
-      __syncwarp();
-      if (qn >= 32) {
-        compute(lane);
+      if (run) {
+        cp_async_wait_prev();
         __syncwarp();
-        if (lane < qn - 32) {
-          qa[w][lane] = qa[w][lane + 32];
-          qo[w][lane] = qo[w][lane + 32];
-          q1[w][lane] = q1[w][lane + 32];
-          q2[w][lane] = q2[w][lane + 32];
-        }
-        __syncwarp();
+        compute((head + lane) & kMask);
+        __syncwarp();  // the slots are free again only after every lane has read them
+        head = (head + 32) & kMask;
         qn -= 32;
       }
+      jc = jn;
+      jn = jnn;
+      ac = an;
     }
-    if (lane < qn)
-      compute(lane);
+    cp_async_wait_all();
+    __syncwarp();
+    for (; qn > 0; qn -= 32, head = (head + 32) & kMask)
+      if (lane < qn)
+        compute((head + lane) & kMask);
   }
+  __shared__ long long wsum[kMxWarps][2];
+  // lane totals, transposed through the warp's own ring (no longer in use)
+  static_assert(32 * (kCols + 1) * sizeof(long long) <= sizeof(ring[0]), "ring too small for the reduction");
+  long long(*red)[kCols + 1] = reinterpret_cast<long long(*)[kCols + 1]>(ring[w]);
+  __syncwarp();
 #pragma unroll
   for (int c = 0; c < kCols; c++)
-    red[w][lane][c] = fx[c];
+    red[lane][c] = fx[c];
   __syncwarp();
   if (lane < kCols) {
     long long t = 0;
     for (int l = 0; l < 32; l++)
-      t += red[w][l][lane];
+      t += red[l][lane];
     if (lane < 9) {
       if (p < a.ngroup)
         a.acc[(size_t) (si0 + lane / 3) * kAccStride + 4 + lane % 3] = t;
@@ -548,7 +576,7 @@ cudaError_t launch_rspace_water(mmnb_handle *h)
   a.rhi2 = h->rhi2;
   a.rlo2 = (float) h->rlo2;
   a.inv_sw = (float) h->inv_sw;
-  a.eta = (float) h->eta;
+  a.pe = (float) (h->eta * kErfcP);
   a.c2 = (float) (h->eta * M_2_SQRTPI);
   a.nel2 = (float) (-h->eta * h->eta * M_LOG2E);
   a.site = h->mx.site;
