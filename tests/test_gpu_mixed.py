@@ -48,6 +48,18 @@ def test_mixed_error_vs_fp64_oracle(n, mesh, seed, fields):
     assert abs(g["elec"] - o["elec"]) < ENERGY_TOL * abs(o["elec"])
 
 
+@pytest.mark.parametrize("order", [2, 3, 4, 5, 6, 7])
+@pytest.mark.parametrize("mesh", [18, 20])
+def test_mixed_p3m_orders(mesh, order):
+    """Every assignment order on two meshes whose sizes are not powers of two."""
+    wb = water_box(6, seed=3)
+    cfg = p3m(wb.box, mesh, p3m_assignment_order=order)
+    g = ElecLJ(precision="mixed", **cfg).init(wb).compute(wb.positions)
+    o = oracle_eval(wb, cfg)
+    assert rel_rms(g["f"], o["f"]) < RMS_TOL
+    assert abs(g["total"] - o["total"]) < ENERGY_TOL * abs(o["total"])
+
+
 def test_mixed_ewald_ksum_c1():
     wb = water_box(6, seed=1)
     cfg = dict(rspace_cutoff=9.0, ewald_screening=0.35, kspace_cutoff=7.0)
