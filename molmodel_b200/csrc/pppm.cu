@@ -383,17 +383,15 @@ cudaError_t launch_p3m_fp64(mmnb_handle *h, const double *d_r)
 // (2^32 units per unit charge), so the mesh, and everything computed from it,
 // is bitwise independent of the order in which sites are spread.
 
+// One thread per site in the caller's order: the position, charge and mask
+// loads are independent and coalesced (no sorted-order indirection in front
+// of them); the fixed-point adds do not depend on the order anyway.
 template <int P>
 __global__ void k_spread_mixed(MeshArgs m, const double *__restrict__ r, const double *__restrict__ q,
-                               const int *__restrict__ mask, const int *__restrict__ sorted,
-                               const int *__restrict__ group, int nslot, int G, unsigned long long *__restrict__ mesh)
+                               const int *__restrict__ mask, int nsite, unsigned long long *__restrict__ mesh)
 {
-  const int sl = blockIdx.x * blockDim.x + threadIdx.x;
-  if (sl >= nslot)
-    return;
-  const int g = sorted[sl / G];
-  const int i = group[2 * g] + sl % G;
-  if (i >= group[2 * g + 1] || !(mask[i] & MMNB_SITE_HAS_Q))
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nsite || !(mask[i] & MMNB_SITE_HAS_Q))
     return;
   const float qi = (float) q[i];
   const double x = r[3 * i], y = r[3 * i + 1], z = r[3 * i + 2];
@@ -454,16 +452,11 @@ __global__ void k_green_to_f32(long nk, const double *__restrict__ green, float 
 }
 
 template <int P>
-__global__ void k_gather_mixed(MeshArgs m, const double *__restrict__ r, const int *__restrict__ sorted,
-                               const int *__restrict__ group, int nslot, int G, const float *__restrict__ mesh,
+__global__ void k_gather_mixed(MeshArgs m, const double *__restrict__ r, int nsite, const float *__restrict__ mesh,
                                long long *__restrict__ acc)
 {
-  const int sl = blockIdx.x * blockDim.x + threadIdx.x;
-  if (sl >= nslot)
-    return;
-  const int g = sorted[sl / G];
-  const int i = group[2 * g] + sl % G;
-  if (i >= group[2 * g + 1])
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nsite)
     return;
   const double x = r[3 * i], y = r[3 * i + 1], z = r[3 * i + 2];
   float W[3][P], ND[3][P];
@@ -523,9 +516,8 @@ static cudaError_t p3m_mixed_p(mmnb_handle *h, const double *d_r)
   const MeshArgs m = mesh_args(h);
   const size_t nr = (size_t) h->mesh[0] * h->mesh[1] * h->mesh[2];
   const long nk = (long) h->mesh[0] * h->mesh[1] * (h->mesh[2] / 2 + 1);
-  const int nslot = h->ngroup * h->G;
-  k_spread_mixed<P><<<div_up(nslot, 128), 128, 0, h->stream>>>(m, d_r, h->d_q, h->d_mask, h->d_sorted, h->d_group,
-                                                               nslot, h->G, h->d_mesh_fx);
+  k_spread_mixed<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->d_q, h->d_mask, h->nsite,
+                                                                   h->d_mesh_fx);
   k_mesh_fx_to_f32<<<div_up((long) nr, 256), 256, 0, h->stream>>>(nr, h->d_mesh_fx, h->d_mesh32);
   timing_mark(h, "p3m_spread");
   if (cufftExecR2C(h->plan_r2c32, h->d_mesh32, h->d_meshk32) != CUFFT_SUCCESS)
@@ -534,8 +526,7 @@ static cudaError_t p3m_mixed_p(mmnb_handle *h, const double *d_r)
   if (cufftExecC2R(h->plan_c2r32, h->d_meshk32, h->d_mesh32) != CUFFT_SUCCESS)
     return cudaErrorUnknown;
   timing_mark(h, "p3m_fft");
-  k_gather_mixed<P><<<div_up(nslot, 128), 128, 0, h->stream>>>(m, d_r, h->d_sorted, h->d_group, nslot, h->G,
-                                                               h->d_mesh32, h->mx.acc);
+  k_gather_mixed<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->nsite, h->d_mesh32, h->mx.acc);
   timing_mark(h, "p3m_gather");
   h->launches += 4;
   return cudaGetLastError();
