@@ -379,6 +379,16 @@ void free_all(mmnb_handle *h)
   for (void *p : ptrs)
     if (p)
       cudaFree(p);
+  if (h->side) {
+    cudaStreamSynchronize(h->side);
+    cudaStreamDestroy(h->side);
+    h->side = nullptr;
+  }
+  if (h->ev_fork)
+    cudaEventDestroy(h->ev_fork);
+  if (h->ev_join)
+    cudaEventDestroy(h->ev_join);
+  h->ev_fork = h->ev_join = nullptr;
   if (h->h_flags)
     cudaFreeHost(h->h_flags);
   if (h->h_f)
@@ -569,6 +579,9 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
   CK(cudaGetDevice(&h->dev));
   CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
   h->stream = h->own_stream;
+  CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
   int s;
   std::vector<int> gvec(h->group);
   if ((s = upload(h, &h->d_group, gvec)) || (s = upload(h, &h->d_excl_ptr, h->excl_ptr)) ||
@@ -758,6 +771,23 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
   const bool mixed = h->cfg.precision == MMNB_MIXED;
   double *energy = d_energy ? d_energy : h->d_energy;
   timing_mark(h, "start");
+  // P3M charge assignment and FFTs depend only on the positions: they run on
+  // the side stream while the list and pair kernels run here, and are joined
+  // back before interpolation (which adds to what the pair kernels wrote).
+  // With stage timing on, the join follows at once so the marks stay serial.
+  const bool p3m = h->any_q && h->cfg.include_kspace && h->p3m;
+  if (p3m) {
+    cudaStream_t main = h->stream;
+    CK(cudaEventRecord(h->ev_fork, main));
+    CK(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+    h->stream = h->side;
+    const cudaError_t e = mixed ? launch_p3m_mixed(h, d_r, 1) : launch_p3m_fp64(h, d_r, 1);
+    h->stream = main;
+    CK(e);
+    CK(cudaEventRecord(h->ev_join, h->side));
+    if (h->timing.on)
+      CK(cudaStreamWaitEvent(main, h->ev_join, 0));
+  }
   CK(launch_gather_anchors(h, d_r));
   CK(launch_rebuild_decide(h, h->force_rebuild_next));
   CK(launch_build_list(h));
@@ -791,11 +821,13 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
     if (mixed)
       CK(cudaMemsetAsync(h->mx.acc, 0, sizeof(long long) * h->nsite * kAccStride, h->stream));
   }
-  if (h->any_q && h->cfg.include_kspace) {
-    if (h->p3m)
-      CK(mixed ? launch_p3m_mixed(h, d_r) : launch_p3m_fp64(h, d_r));
-    else if (h->kspace)
-      CK(launch_kspace(h, d_r));
+  if (p3m) {
+    if (!h->timing.on)
+      CK(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+    CK(mixed ? launch_p3m_mixed(h, d_r, 2) : launch_p3m_fp64(h, d_r, 2));
+    timing_mark(h, "kspace");
+  } else if (h->any_q && h->cfg.include_kspace && h->kspace) {
+    CK(launch_kspace(h, d_r));
     timing_mark(h, "kspace");
   }
   CK(launch_finalize(h, d_f, energy));

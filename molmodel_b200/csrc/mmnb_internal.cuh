@@ -71,6 +71,10 @@ struct mmnb_handle {
   int dev = 0;
   cudaStream_t stream = nullptr;       // stream every launch goes to
   cudaStream_t own_stream = nullptr;   // created by mmnb_create, destroyed by mmnb_destroy
+  // P3M charge assignment and FFTs run on `side`, forked from and joined back
+  // into `stream`, concurrently with the list and pair kernels
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::string err;
 
   // derived settings
@@ -198,8 +202,9 @@ cudaError_t launch_rspace_mixed(mmnb_handle *h);
 cudaError_t launch_rspace_water(mmnb_handle *h);
 cudaError_t launch_exclusions(mmnb_handle *h, const double *d_r);
 cudaError_t launch_p3m_green(mmnb_handle *h);
-cudaError_t launch_p3m_fp64(mmnb_handle *h, const double *d_r);
-cudaError_t launch_p3m_mixed(mmnb_handle *h, const double *d_r);
+// stage bit 1: spread + FFT round trip, bit 2: gather
+cudaError_t launch_p3m_fp64(mmnb_handle *h, const double *d_r, int stage);
+cudaError_t launch_p3m_mixed(mmnb_handle *h, const double *d_r, int stage);
 cudaError_t launch_green32(mmnb_handle *h);
 cudaError_t launch_kspace(mmnb_handle *h, const double *d_r);
 cudaError_t launch_finalize(mmnb_handle *h, double *d_f, double *d_energy);

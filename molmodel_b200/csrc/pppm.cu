@@ -334,45 +334,53 @@ static MeshArgs mesh_args(mmnb_handle *h)
   return m;
 }
 
+// stage bit 1: charge assignment and the FFT round trip; bit 2: interpolation
 template <int P>
-static cudaError_t p3m_fp64_p(mmnb_handle *h, const double *d_r)
+static cudaError_t p3m_fp64_p(mmnb_handle *h, const double *d_r, int stage)
 {
   const MeshArgs m = mesh_args(h);
   const size_t nr = (size_t) h->mesh[0] * h->mesh[1] * h->mesh[2];
   const long nk = (long) h->mesh[0] * h->mesh[1] * (h->mesh[2] / 2 + 1);
-  cudaError_t e = cudaMemsetAsync(h->d_mesh, 0, sizeof(double) * nr, h->stream);
-  if (e != cudaSuccess)
-    return e;
-  k_spread_fp64<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->d_q, h->d_mask, h->d_mesh);
-  timing_mark(h, "p3m_spread");
-  if (cufftExecD2Z(h->plan_r2c, h->d_mesh, h->d_meshk) != CUFFT_SUCCESS)
-    return cudaErrorUnknown;
   const bool ik = h->cfg.p3m_ik_differentiate != 0;
-  k_green_mul<<<div_up(nk, 256), 256, 0, h->stream>>>(nk, h->d_green, h->d_meshk, h->d_kvec,
-                                                      ik ? h->d_egridk : nullptr);
-  if (ik)
-    for (int d = 0; d < 3; d++)
-      if (cufftExecZ2D(h->plan_c2r, h->d_egridk + d * nk, h->d_egrid + d * nr) != CUFFT_SUCCESS)
-        return cudaErrorUnknown;
-  if (cufftExecZ2D(h->plan_c2r, h->d_meshk, h->d_mesh) != CUFFT_SUCCESS)
-    return cudaErrorUnknown;
-  timing_mark(h, "p3m_fft");
-  k_gather_fp64<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->d_mesh, ik ? h->d_egrid : nullptr,
-                                                                 nr, h->d_phi, h->d_evec);
-  timing_mark(h, "p3m_gather");
-  h->launches += 3;
+  if (stage & 1) {
+    cudaError_t e = cudaMemsetAsync(h->d_mesh, 0, sizeof(double) * nr, h->stream);
+    if (e != cudaSuccess)
+      return e;
+    k_spread_fp64<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->d_q, h->d_mask, h->d_mesh);
+    timing_mark(h, "p3m_spread");
+    if (cufftSetStream(h->plan_r2c, h->stream) != CUFFT_SUCCESS ||
+        cufftSetStream(h->plan_c2r, h->stream) != CUFFT_SUCCESS ||
+        cufftExecD2Z(h->plan_r2c, h->d_mesh, h->d_meshk) != CUFFT_SUCCESS)
+      return cudaErrorUnknown;
+    k_green_mul<<<div_up(nk, 256), 256, 0, h->stream>>>(nk, h->d_green, h->d_meshk, h->d_kvec,
+                                                        ik ? h->d_egridk : nullptr);
+    if (ik)
+      for (int d = 0; d < 3; d++)
+        if (cufftExecZ2D(h->plan_c2r, h->d_egridk + d * nk, h->d_egrid + d * nr) != CUFFT_SUCCESS)
+          return cudaErrorUnknown;
+    if (cufftExecZ2D(h->plan_c2r, h->d_meshk, h->d_mesh) != CUFFT_SUCCESS)
+      return cudaErrorUnknown;
+    timing_mark(h, "p3m_fft");
+    h->launches += 2;
+  }
+  if (stage & 2) {
+    k_gather_fp64<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->d_mesh, ik ? h->d_egrid : nullptr,
+                                                                   nr, h->d_phi, h->d_evec);
+    timing_mark(h, "p3m_gather");
+    h->launches += 1;
+  }
   return cudaGetLastError();
 }
 
-cudaError_t launch_p3m_fp64(mmnb_handle *h, const double *d_r)
+cudaError_t launch_p3m_fp64(mmnb_handle *h, const double *d_r, int stage)
 {
   switch (h->cfg.p3m_assignment_order) {
-  case 2: return p3m_fp64_p<2>(h, d_r);
-  case 3: return p3m_fp64_p<3>(h, d_r);
-  case 4: return p3m_fp64_p<4>(h, d_r);
-  case 5: return p3m_fp64_p<5>(h, d_r);
-  case 6: return p3m_fp64_p<6>(h, d_r);
-  case 7: return p3m_fp64_p<7>(h, d_r);
+  case 2: return p3m_fp64_p<2>(h, d_r, stage);
+  case 3: return p3m_fp64_p<3>(h, d_r, stage);
+  case 4: return p3m_fp64_p<4>(h, d_r, stage);
+  case 5: return p3m_fp64_p<5>(h, d_r, stage);
+  case 6: return p3m_fp64_p<6>(h, d_r, stage);
+  case 7: return p3m_fp64_p<7>(h, d_r, stage);
   default: return cudaErrorInvalidValue;
   }
 }
@@ -511,36 +519,43 @@ cudaError_t launch_green32(mmnb_handle *h)
 }
 
 template <int P>
-static cudaError_t p3m_mixed_p(mmnb_handle *h, const double *d_r)
+static cudaError_t p3m_mixed_p(mmnb_handle *h, const double *d_r, int stage)
 {
   const MeshArgs m = mesh_args(h);
   const size_t nr = (size_t) h->mesh[0] * h->mesh[1] * h->mesh[2];
   const long nk = (long) h->mesh[0] * h->mesh[1] * (h->mesh[2] / 2 + 1);
-  k_spread_mixed<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->d_q, h->d_mask, h->nsite,
-                                                                   h->d_mesh_fx);
-  k_mesh_fx_to_f32<<<div_up((long) nr, 256), 256, 0, h->stream>>>(nr, h->d_mesh_fx, h->d_mesh32);
-  timing_mark(h, "p3m_spread");
-  if (cufftExecR2C(h->plan_r2c32, h->d_mesh32, h->d_meshk32) != CUFFT_SUCCESS)
-    return cudaErrorUnknown;
-  k_green_mul32<<<div_up(nk, 256), 256, 0, h->stream>>>(nk, h->d_green32, h->d_meshk32);
-  if (cufftExecC2R(h->plan_c2r32, h->d_meshk32, h->d_mesh32) != CUFFT_SUCCESS)
-    return cudaErrorUnknown;
-  timing_mark(h, "p3m_fft");
-  k_gather_mixed<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->nsite, h->d_mesh32, h->mx.acc);
-  timing_mark(h, "p3m_gather");
-  h->launches += 4;
+  if (stage & 1) {
+    k_spread_mixed<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->d_q, h->d_mask, h->nsite,
+                                                                     h->d_mesh_fx);
+    k_mesh_fx_to_f32<<<div_up((long) nr, 256), 256, 0, h->stream>>>(nr, h->d_mesh_fx, h->d_mesh32);
+    timing_mark(h, "p3m_spread");
+    if (cufftSetStream(h->plan_r2c32, h->stream) != CUFFT_SUCCESS ||
+        cufftSetStream(h->plan_c2r32, h->stream) != CUFFT_SUCCESS ||
+        cufftExecR2C(h->plan_r2c32, h->d_mesh32, h->d_meshk32) != CUFFT_SUCCESS)
+      return cudaErrorUnknown;
+    k_green_mul32<<<div_up(nk, 256), 256, 0, h->stream>>>(nk, h->d_green32, h->d_meshk32);
+    if (cufftExecC2R(h->plan_c2r32, h->d_meshk32, h->d_mesh32) != CUFFT_SUCCESS)
+      return cudaErrorUnknown;
+    timing_mark(h, "p3m_fft");
+    h->launches += 3;
+  }
+  if (stage & 2) {
+    k_gather_mixed<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->nsite, h->d_mesh32, h->mx.acc);
+    timing_mark(h, "p3m_gather");
+    h->launches += 1;
+  }
   return cudaGetLastError();
 }
 
-cudaError_t launch_p3m_mixed(mmnb_handle *h, const double *d_r)
+cudaError_t launch_p3m_mixed(mmnb_handle *h, const double *d_r, int stage)
 {
   switch (h->cfg.p3m_assignment_order) {
-  case 2: return p3m_mixed_p<2>(h, d_r);
-  case 3: return p3m_mixed_p<3>(h, d_r);
-  case 4: return p3m_mixed_p<4>(h, d_r);
-  case 5: return p3m_mixed_p<5>(h, d_r);
-  case 6: return p3m_mixed_p<6>(h, d_r);
-  case 7: return p3m_mixed_p<7>(h, d_r);
+  case 2: return p3m_mixed_p<2>(h, d_r, stage);
+  case 3: return p3m_mixed_p<3>(h, d_r, stage);
+  case 4: return p3m_mixed_p<4>(h, d_r, stage);
+  case 5: return p3m_mixed_p<5>(h, d_r, stage);
+  case 6: return p3m_mixed_p<6>(h, d_r, stage);
+  case 7: return p3m_mixed_p<7>(h, d_r, stage);
   default: return cudaErrorInvalidValue;
   }
 }
