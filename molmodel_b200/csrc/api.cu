@@ -375,7 +375,7 @@ void free_all(mmnb_handle *h)
                   h->d_phi, h->d_evec, h->d_ljf, h->d_lj_part, h->d_elec_part, h->d_energy, h->d_r, h->d_f,
                   h->d_mesh, h->d_meshk, h->d_green, h->d_kvec, h->d_egrid, h->d_egridk, h->d_mesh32,
                   h->d_meshk32, h->d_green32, h->d_mesh_fx, h->d_kint, h->d_kvecs, h->d_ak, h->d_skc,
-                  h->mx.site, h->mx.par, h->mx.anchor, h->mx.lj, h->mx.acc, h->d_ep_part};
+                  h->mx.site, h->mx.par, h->mx.anchor, h->mx.lj, h->mx.acc, h->d_wsum};
   for (void *p : ptrs)
     if (p)
       cudaFree(p);
@@ -615,13 +615,15 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
   if ((s = dalloc(h, &h->d_phi, nsite)) || (s = dalloc(h, &h->d_evec, 3 * (size_t) nsite)) ||
       (s = dalloc(h, &h->d_ljf, 3 * (size_t) nsite)) || (s = dalloc(h, &h->d_lj_part, nlj)) ||
       (s = dalloc(h, &h->d_elec_part, h->elec_blocks)) || (s = dalloc(h, &h->d_energy, 8)) ||
-      (s = dalloc(h, &h->d_r, 3 * (size_t) nsite)) || (s = dalloc(h, &h->d_f, 3 * (size_t) nsite)))
+      (s = dalloc(h, &h->d_r, 3 * (size_t) nsite)) || (s = dalloc(h, &h->d_f, 3 * (size_t) nsite)) ||
+      (s = dalloc(h, &h->d_wsum, 4)))
     return s;
   CK(cudaMemset(h->d_lj_part, 0, sizeof(double) * nlj));
+  CK(cudaMemset(h->d_wsum, 0, sizeof(unsigned long long) * 4));
   if (c->precision == MMNB_MIXED) {
     if ((s = dalloc(h, &h->mx.site, nslot)) || (s = dalloc(h, &h->mx.par, nslot)) ||
         (s = dalloc(h, &h->mx.anchor, ngroup)) || (s = dalloc(h, &h->mx.lj, ngroup)) ||
-        (s = dalloc(h, &h->mx.acc, (size_t) nsite * kAccStride)) || (s = dalloc(h, &h->d_ep_part, h->lj_pair_blocks)))
+        (s = dalloc(h, &h->mx.acc, (size_t) nsite * kAccStride)))
       return s;
     CK(cudaMemset(h->mx.acc, 0, sizeof(long long) * nsite * kAccStride));
   }
@@ -776,12 +778,31 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
   // back before interpolation (which adds to what the pair kernels wrote).
   // With stage timing on, the join follows at once so the marks stay serial.
   const bool p3m = h->any_q && h->cfg.include_kspace && h->p3m;
+  // the mixed form's FP64 site arrays (zeroed here, then the exclusion
+  // corrections) do not meet the pair kernels either: they go to the side
+  // stream too
+  const bool excl_side = p3m && mixed && h->cfg.include_rspace;
+  auto zero_site_arrays = [&]() -> cudaError_t {
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(h->d_phi, 0, sizeof(double) * h->nsite, h->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->d_evec, 0, sizeof(double) * 3 * h->nsite, h->stream)) != cudaSuccess)
+      return e;
+    return cudaMemsetAsync(h->d_ljf, 0, sizeof(double) * 3 * h->nsite, h->stream);
+  };
   if (p3m) {
     cudaStream_t main = h->stream;
     CK(cudaEventRecord(h->ev_fork, main));
     CK(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
     h->stream = h->side;
-    const cudaError_t e = mixed ? launch_p3m_mixed(h, d_r, 1) : launch_p3m_fp64(h, d_r, 1);
+    cudaError_t e = cudaSuccess;
+    if (excl_side) {
+      e = zero_site_arrays();
+      if (e == cudaSuccess)
+        e = launch_exclusions(h, d_r);
+      timing_mark(h, "rspace_excl");
+    }
+    if (e == cudaSuccess)
+      e = mixed ? launch_p3m_mixed(h, d_r, 1) : launch_p3m_fp64(h, d_r, 1);
     h->stream = main;
     CK(e);
     CK(cudaEventRecord(h->ev_join, h->side));
@@ -792,12 +813,9 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
   CK(launch_rebuild_decide(h, h->force_rebuild_next));
   CK(launch_build_list(h));
   timing_mark(h, "nbrlist");
-  if (mixed || !h->cfg.include_rspace) {
-    // FP64 site arrays collect the terms the fixed-point sums do not hold
-    CK(cudaMemsetAsync(h->d_phi, 0, sizeof(double) * h->nsite, h->stream));
-    CK(cudaMemsetAsync(h->d_evec, 0, sizeof(double) * 3 * h->nsite, h->stream));
-    CK(cudaMemsetAsync(h->d_ljf, 0, sizeof(double) * 3 * h->nsite, h->stream));
-  }
+  // FP64 site arrays collect the terms the fixed-point sums do not hold
+  if ((mixed || !h->cfg.include_rspace) && !excl_side)
+    CK(zero_site_arrays());
   if (mixed)
     CK(launch_prep_mixed(h, d_r));
   else
@@ -814,8 +832,10 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
       CK(launch_rspace_fp64(h));
     }
     timing_mark(h, "rspace_pair");
-    CK(launch_exclusions(h, d_r));
-    timing_mark(h, "rspace_excl");
+    if (!excl_side) {
+      CK(launch_exclusions(h, d_r));
+      timing_mark(h, "rspace_excl");
+    }
   } else {
     CK(cudaMemsetAsync(h->d_lj_part, 0, sizeof(double) * (h->lj_pair_blocks + h->lj_excl_blocks), h->stream));
     if (mixed)

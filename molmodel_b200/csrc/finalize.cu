@@ -3,15 +3,15 @@
 // Per site: phi -= (2 eta / sqrt(pi)) q, plus the neutralising background
 // -pi/(eta^2 V) sum(q) when the system is charged; F += q E + F_LJ (AtomSite
 // projection, include/eleclj.hpp:68-71).  Energies: elec = (q . phi)/2 and
-// LJ = pair sum + tail, reduced in a fixed order (per-block partials, then one
-// block), so the FP64 energies are bitwise reproducible.
+// LJ = pair sum + tail.  Each block writes its partial sum; the last block to
+// finish (a counter taken after a fence) adds the partials in index order, so
+// the FP64 energies are bitwise reproducible without a second launch.
 
 #include "mmnb_internal.cuh"
 
 namespace mmnb {
 
 constexpr int kFinThreads = 256;
-constexpr int kEnergyThreads = 1024;
 
 struct FinArgs {
   int nsite, do_self;
@@ -19,11 +19,33 @@ struct FinArgs {
   const double *q;
   const long long *acc;  // mixed form: fixed-point potential, field and LJ force per site
   double *phi, *evec, *ljf, *f, *elec_part;
+  // energy reduction
+  const double *lj_part;              // per-block LJ partials [lj_lo, lj_hi)
+  int lj_lo, lj_hi, any_q;
+  const unsigned long long *wsum;     // water kernel's fixed-point pair energies, or null
+  unsigned long long *counter;        // finished-block counter, left at 0
+  double tail;
+  double *energy;
 };
 
-__global__ void k_finalize(FinArgs a)
+__device__ __forceinline__ double block_sum(double v, double *sh)
+{
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  const double t = sh[0];
+  __syncthreads();
+  return t;
+}
+
+__global__ void __launch_bounds__(kFinThreads) k_finalize(FinArgs a)
 {
   __shared__ double se[kFinThreads];
+  __shared__ bool last;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double e = 0;
   if (i < a.nsite) {
@@ -50,50 +72,36 @@ __global__ void k_finalize(FinArgs a)
       a.f[3 * i + 2] += qi * a.evec[3 * i + 2] + a.ljf[3 * i + 2];
     }
   }
-  se[threadIdx.x] = e;
-  __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s)
-      se[threadIdx.x] += se[threadIdx.x + s];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0)
-    a.elec_part[blockIdx.x] = se[0];
-}
-
-// elec = (q . phi)/2 over the site potentials, plus the real-space Coulomb
-// energy summed directly by the rigid-water kernel (nep partials, already in
-// final units; 0 when another pair kernel filled the site potentials)
-__global__ void __launch_bounds__(kEnergyThreads) k_energy(int nelec, const double *__restrict__ elec_part, int nlj,
-                                                           const double *__restrict__ lj_part, int nep,
-                                                           const double *__restrict__ ep_part, double tail, int any_q,
-                                                           double *__restrict__ energy)
-{
-  __shared__ double se[kEnergyThreads], sl[kEnergyThreads];
-  double e = 0, l = 0;
-  for (int i = threadIdx.x; i < nelec; i += blockDim.x)
-    e += elec_part[i];
-  for (int i = threadIdx.x; i < nep; i += blockDim.x)
-    e += 2 * ep_part[i];
-  for (int i = threadIdx.x; i < nlj; i += blockDim.x)
-    l += lj_part[i];
-  se[threadIdx.x] = e;
-  sl[threadIdx.x] = l;
-  __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s) {
-      se[threadIdx.x] += se[threadIdx.x + s];
-      sl[threadIdx.x] += sl[threadIdx.x + s];
-    }
-    __syncthreads();
-  }
+  const double bs = block_sum(e, se);
   if (threadIdx.x == 0) {
-    const double elec = any_q ? se[0] / 2 : 0;
-    const double lj = sl[0] + tail;
-    energy[0] = elec;
-    energy[1] = lj;
-    energy[2] = tail;
-    energy[3] = elec + lj;
+    a.elec_part[blockIdx.x] = bs;
+    __threadfence();
+    last = atomicAdd(a.counter, 1ull) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last)
+    return;
+  __threadfence();
+  double el = 0, lj = 0;
+  for (int k = threadIdx.x; k < (int) gridDim.x; k += blockDim.x)
+    el += a.elec_part[k];
+  for (int k = a.lj_lo + threadIdx.x; k < a.lj_hi; k += blockDim.x)
+    lj += a.lj_part[k];
+  el = block_sum(el, se);
+  lj = block_sum(lj, se);
+  if (threadIdx.x == 0) {
+    if (a.wsum) {
+      // the water kernel's real-space Coulomb energy is a pair sum (not in phi)
+      el += 2 * ((double) (long long) a.wsum[0] * kFxInv);
+      lj += (double) (long long) a.wsum[1] * kFxInv;
+    }
+    const double elec = a.any_q ? el / 2 : 0;
+    const double ljt = lj + a.tail;
+    a.energy[0] = elec;
+    a.energy[1] = ljt;
+    a.energy[2] = a.tail;
+    a.energy[3] = elec + ljt;
+    *a.counter = 0ull;
   }
 }
 
@@ -112,13 +120,18 @@ cudaError_t launch_finalize(mmnb_handle *h, double *d_f, double *d_energy)
   a.ljf = h->d_ljf;
   a.f = d_f;
   a.elec_part = h->d_elec_part;
+  a.lj_part = h->d_lj_part;
+  // the water kernel leaves its LJ energy in the fixed-point word, not in the
+  // pair partials
+  a.lj_lo = h->used_water ? h->lj_pair_blocks : 0;
+  a.lj_hi = h->lj_pair_blocks + h->lj_excl_blocks;
+  a.any_q = h->any_q ? 1 : 0;
+  a.wsum = h->used_water ? h->d_wsum : nullptr;
+  a.counter = h->d_wsum + 2;
+  a.tail = h->cfg.include_lj_correction ? h->lj_correction : 0.0;
+  a.energy = d_energy;
   k_finalize<<<h->elec_blocks, kFinThreads, 0, h->stream>>>(a);
-  const int nlj = h->lj_pair_blocks + h->lj_excl_blocks;
-  k_energy<<<1, kEnergyThreads, 0, h->stream>>>(h->elec_blocks, h->d_elec_part, nlj, h->d_lj_part,
-                                                 h->used_water ? h->lj_pair_blocks : 0, h->d_ep_part,
-                                             h->cfg.include_lj_correction ? h->lj_correction : 0.0,
-                                             h->any_q ? 1 : 0, d_energy);
-  h->launches += 2;
+  h->launches += 1;
   return cudaGetLastError();
 }
 

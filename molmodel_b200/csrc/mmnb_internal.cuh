@@ -143,7 +143,9 @@ struct mmnb_handle {
   // outputs (original order)
   double *d_phi = nullptr, *d_evec = nullptr, *d_ljf = nullptr;
   double *d_lj_part = nullptr;       // LJ energy partials: pair-kernel blocks, then exclusion blocks
-  double *d_ep_part = nullptr;       // real-space Coulomb energy partials of the water kernel
+  // [0], [1]: fixed-point Coulomb and LJ pair energies of the water kernel;
+  // [2]: block counter of the finalize kernel's last-block reduction
+  unsigned long long *d_wsum = nullptr;
   int lj_pair_blocks = 0, lj_excl_blocks = 0;
   double *d_elec_part = nullptr;     // per block
   int elec_blocks = 0;

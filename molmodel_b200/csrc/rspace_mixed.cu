@@ -350,7 +350,7 @@ struct WaterArgs {
   const double4 *anchor;
   const int *nbr, *nbr_count, *sorted, *group;
   long long *acc;         // per site: slots 4..6 receive the force, 0..3 are cleared
-  double *lj_part, *ep_part;
+  unsigned long long *wsum;  // fixed-point Coulomb and LJ pair energies, zeroed by the prep kernel
 };
 
 // One site pair of a water group pair: adds q_j b1 S d to the row site's field
@@ -561,8 +561,9 @@ __global__ void __launch_bounds__(kMxWarps * 32, 4) k_pair_water(WaterArgs a)
       te += wsum[k][0];
       tl += wsum[k][1];
     }
-    a.ep_part[blockIdx.x] = (double) te * kFxInv;
-    a.lj_part[blockIdx.x] = (double) tl * kFxInv;
+    // integer sums: the totals do not depend on the order blocks finish in
+    atomicAdd(a.wsum, (unsigned long long) te);
+    atomicAdd(a.wsum + 1, (unsigned long long) tl);
   }
 }
 
@@ -587,8 +588,7 @@ cudaError_t launch_rspace_water(mmnb_handle *h)
   a.sorted = h->d_sorted;
   a.group = h->d_group;
   a.acc = h->mx.acc;
-  a.lj_part = h->d_lj_part;
-  a.ep_part = h->d_ep_part;
+  a.wsum = h->d_wsum;
   k_pair_water<<<pair_blocks(h), kMxWarps * 32, 0, h->stream>>>(a);
   h->launches += 1;
   return cudaGetLastError();
@@ -601,9 +601,11 @@ __global__ void k_prep_mixed(const double *__restrict__ r, const double *__restr
                              const double *__restrict__ rscreen, const int *__restrict__ mask,
                              const int *__restrict__ sorted, const int *__restrict__ group, int ngroup, int G,
                              float4 *__restrict__ site, float4 *__restrict__ par, double4 *__restrict__ anchor,
-                             float2 *__restrict__ lj)
+                             float2 *__restrict__ lj, unsigned long long *__restrict__ wsum)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < 2)
+    wsum[s] = 0ull;
   if (s < ngroup * G) {
     const int p = s / G, k = s % G;
     const int g = sorted[p];
@@ -631,7 +633,7 @@ cudaError_t launch_prep_mixed(mmnb_handle *h, const double *d_r)
   const int n = h->ngroup * h->G;
   k_prep_mixed<<<div_up(n, 256), 256, 0, h->stream>>>(d_r, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_mask,
                                                       h->d_sorted, h->d_group, h->ngroup, h->G, h->mx.site,
-                                                      h->mx.par, h->mx.anchor, h->mx.lj);
+                                                      h->mx.par, h->mx.anchor, h->mx.lj, h->d_wsum);
   h->launches += 1;
   return cudaGetLastError();
 }
