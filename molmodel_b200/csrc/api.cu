@@ -809,9 +809,8 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
     if (h->timing.on)
       CK(cudaStreamWaitEvent(main, h->ev_join, 0));
   }
-  CK(launch_gather_anchors(h, d_r));
-  CK(launch_rebuild_decide(h, h->force_rebuild_next));
-  CK(launch_build_list(h));
+  CK(launch_list_check(h, d_r, h->force_rebuild_next));
+  CK(launch_list_rebuild(h));
   timing_mark(h, "nbrlist");
   // FP64 site arrays collect the terms the fixed-point sums do not hold
   if ((mixed || !h->cfg.include_rspace) && !excl_side)

@@ -124,6 +124,7 @@ struct mmnb_handle {
   double *d_anchor_sorted = nullptr; // 3*ngroup anchors at the last rebuild, sorted order
   double *d_top2 = nullptr;          // per-block top-2 displacements
   int top2_blocks = 0;
+  int rebuild_grid = 0;              // blocks of the cooperative rebuild launch (0: not sized yet)
   int rowcap = 0;
   int *d_nbr = nullptr;              // ngroup * rowcap, sorted positions
   int *d_nbr_count = nullptr;        // ngroup
@@ -194,9 +195,9 @@ struct mmnb_handle {
 namespace mmnb {
 
 // ---- launchers (defined in the .cu files) ----------------------------------
-cudaError_t launch_gather_anchors(mmnb_handle *h, const double *d_r);
-cudaError_t launch_rebuild_decide(mmnb_handle *h, int force);
-cudaError_t launch_build_list(mmnb_handle *h);
+// anchors, rebuild decision; then the rebuild (a no-op launch when not due)
+cudaError_t launch_list_check(mmnb_handle *h, const double *d_r, int force);
+cudaError_t launch_list_rebuild(mmnb_handle *h);
 cudaError_t launch_sort_sites(mmnb_handle *h, const double *d_r);
 cudaError_t launch_rspace_fp64(mmnb_handle *h);
 cudaError_t launch_prep_mixed(mmnb_handle *h, const double *d_r);

@@ -21,6 +21,8 @@
 // kernels accumulate on their own rows only, without atomics.  Rows are
 // indexed by sorted position (groups ordered by the Morton rank of their cell).
 
+#include <cooperative_groups.h>
+
 #include "mmnb_internal.cuh"
 
 namespace mmnb {
@@ -36,18 +38,6 @@ __device__ __forceinline__ double exact_sq3(double x, double y, double z)
   return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
 }
 
-__global__ void k_gather_anchors(const double *__restrict__ r, const int *__restrict__ group, int ngroup,
-                                 double *__restrict__ anchor)
-{
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= ngroup)
-    return;
-  const int a = group[2 * g];
-  anchor[3 * g] = r[3 * a];
-  anchor[3 * g + 1] = r[3 * a + 1];
-  anchor[3 * g + 2] = r[3 * a + 2];
-}
-
 // merge two (largest, second largest) pairs of a multiset
 __device__ __forceinline__ void top2_merge(double &a, double &b, double a2, double b2)
 {
@@ -56,17 +46,52 @@ __device__ __forceinline__ void top2_merge(double &a, double &b, double a2, doub
   a = hi;
 }
 
-constexpr int kTop2Threads = 256;
+constexpr int kCheckThreads = 256;
 
-__global__ void k_top2(const double *__restrict__ anchor, const double *__restrict__ last, int n,
-                       double *__restrict__ partial)
+__device__ __forceinline__ void block_top2(double &a, double &b, double *sa, double *sb)
 {
-  __shared__ double sa[kTop2Threads], sb[kTop2Threads];
+  sa[threadIdx.x] = a;
+  sb[threadIdx.x] = b;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      double x = sa[threadIdx.x], y = sb[threadIdx.x];
+      top2_merge(x, y, sa[threadIdx.x + s], sb[threadIdx.x + s]);
+      sa[threadIdx.x] = x;
+      sb[threadIdx.x] = y;
+    }
+    __syncthreads();
+  }
+  a = sa[0];
+  b = sb[0];
+}
+
+// Anchors of this evaluation, the two largest anchor moves since the last
+// build, and the rebuild decision (first || forced || largest + second >
+// width || fixed interval), all in one launch: each block reduces its share,
+// the last block to finish merges the block results.  On a rebuild the last
+// block also clears the cell counts for the rebuild kernel.
+// flags[4] counts evaluations, flags[5] rebuilds, flags[6] is the block counter.
+__global__ void __launch_bounds__(kCheckThreads) k_list_check(const double *__restrict__ r,
+                                                              const int *__restrict__ group, int ngroup,
+                                                              const double *__restrict__ last, double width,
+                                                              int first, int force, int interval,
+                                                              double *__restrict__ anchor,
+                                                              double *__restrict__ partial, int *__restrict__ flags,
+                                                              int *__restrict__ cell_count, int ncell3)
+{
+  __shared__ double sa[kCheckThreads], sb[kCheckThreads];
+  __shared__ bool last_block;
   double a = 0, b = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double dx = __dsub_rn(anchor[3 * i], last[3 * i]);
-    const double dy = __dsub_rn(anchor[3 * i + 1], last[3 * i + 1]);
-    const double dz = __dsub_rn(anchor[3 * i + 2], last[3 * i + 2]);
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroup; g += gridDim.x * blockDim.x) {
+    const int s0 = group[2 * g];
+    const double x = r[3 * s0], y = r[3 * s0 + 1], z = r[3 * s0 + 2];
+    anchor[3 * g] = x;
+    anchor[3 * g + 1] = y;
+    anchor[3 * g + 2] = z;
+    const double dx = __dsub_rn(x, last[3 * g]);
+    const double dy = __dsub_rn(y, last[3 * g + 1]);
+    const double dz = __dsub_rn(z, last[3 * g + 2]);
     const double d = __dsqrt_rn(exact_sq3(dx, dy, dz));
     if (d > a) {
       b = a;
@@ -75,101 +100,88 @@ __global__ void k_top2(const double *__restrict__ anchor, const double *__restri
       b = d;
     }
   }
-  sa[threadIdx.x] = a;
-  sb[threadIdx.x] = b;
-  __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s) {
-      double x = sa[threadIdx.x], y = sb[threadIdx.x];
-      top2_merge(x, y, sa[threadIdx.x + s], sb[threadIdx.x + s]);
-      sa[threadIdx.x] = x;
-      sb[threadIdx.x] = y;
-    }
-    __syncthreads();
-  }
+  block_top2(a, b, sa, sb);
   if (threadIdx.x == 0) {
-    partial[2 * blockIdx.x] = sa[0];
-    partial[2 * blockIdx.x + 1] = sb[0];
+    partial[2 * blockIdx.x] = a;
+    partial[2 * blockIdx.x + 1] = b;
+    __threadfence();
+    last_block = atomicAdd(flags + 6, 1) == (int) gridDim.x - 1;
   }
-}
-
-// flags[kFlagRebuild] = first || forced || largest + second > width.
-// flags[4] counts evaluations for the fixed-interval mode.
-__global__ void k_decide(const double *__restrict__ partial, int nblocks, double width, int first,
-                         int force, int interval, int *__restrict__ flags)
-{
-  __shared__ double sa[kTop2Threads], sb[kTop2Threads];
-  double a = 0, b = 0;
-  for (int i = threadIdx.x; i < nblocks; i += blockDim.x)
-    top2_merge(a, b, partial[2 * i], partial[2 * i + 1]);
-  sa[threadIdx.x] = a;
-  sb[threadIdx.x] = b;
   __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s) {
-      double x = sa[threadIdx.x], y = sb[threadIdx.x];
-      top2_merge(x, y, sa[threadIdx.x + s], sb[threadIdx.x + s]);
-      sa[threadIdx.x] = x;
-      sb[threadIdx.x] = y;
-    }
-    __syncthreads();
-  }
+  if (!last_block)
+    return;
+  __threadfence();
+  a = b = 0;
+  for (int i = threadIdx.x; i < (int) gridDim.x; i += blockDim.x)
+    top2_merge(a, b, partial[2 * i], partial[2 * i + 1]);
+  block_top2(a, b, sa, sb);
+  __shared__ int rebuild_s;
   if (threadIdx.x == 0) {
     const int count = flags[4];
-    int rebuild = first || force || (__dadd_rn(sb[0], sa[0]) > width);
+    int rebuild = first || force || (__dadd_rn(b, a) > width);
     if (interval > 0 && count % interval == 0)
       rebuild = 1;
     flags[kFlagRebuild] = rebuild;
     flags[4] = count + 1;
     if (rebuild)
       flags[5] += 1;  // rebuild counter
+    flags[6] = 0;
+    rebuild_s = rebuild;
   }
+  __syncthreads();
+  if (rebuild_s)
+    for (int c = threadIdx.x; c < ncell3; c += blockDim.x)
+      cell_count[c] = 0;
 }
 
-__global__ void k_cell_assign(const double *__restrict__ anchor, int ngroup, CellGeom cg,
-                              const int *__restrict__ cell_rank, const int *__restrict__ flags,
-                              int *__restrict__ cell_of_group, int *__restrict__ cell_count,
-                              int *__restrict__ slot, double *__restrict__ last)
+struct RebuildArgs {
+  int ngroup, ncell3, nstencil, rowcap;
+  CellGeom cg;
+  Box box;
+  const double *anchor;      // this evaluation's anchors (original order)
+  const int *cell_rank;      // reference cell index -> Morton rank
+  const int *stencil;        // 3 per offset, components in [0, n)
+  int *flags;
+  int *cell_of_group, *cell_count, *slot, *start, *sorted, *rank;
+  double *last, *anchor_sorted;
+  int *nbr, *nbr_count;
+};
+
+constexpr int kRebuildThreads = 256;
+constexpr int kBuildWarps = kRebuildThreads / 32;
+
+// cell = round(x / l_cell) mod n per axis; the anchors become the new "last"
+__device__ __forceinline__ void cell_assign(const RebuildArgs &a, int g)
 {
-  if (!flags[kFlagRebuild])
-    return;
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= ngroup)
-    return;
-  const int n = cg.n;
+  const int n = a.cg.n;
   int ijk[3];
   for (int d = 0; d < 3; d++) {
-    const double x = anchor[3 * g + d];
-    ijk[d] = (int) floor(__dadd_rn(__ddiv_rn(x, cg.lc[d]), 0.5));
+    const double x = a.anchor[3 * g + d];
+    ijk[d] = (int) floor(__dadd_rn(__ddiv_rn(x, a.cg.lc[d]), 0.5));
     ijk[d] %= n;
     if (ijk[d] < 0)
       ijk[d] += n;
-    last[3 * g + d] = x;
+    a.last[3 * g + d] = x;
   }
   const int c = (ijk[0] * n + ijk[1]) * n + ijk[2];
-  cell_of_group[g] = c;
-  slot[g] = atomicAdd(&cell_count[cell_rank[c]], 1);
+  a.cell_of_group[g] = c;
+  a.slot[g] = atomicAdd(&a.cell_count[a.cell_rank[c]], 1);
 }
 
-// exclusive scan of per-rank counts, one block
-constexpr int kScanThreads = 1024;
-
-__global__ void k_scan_cells(const int *__restrict__ count, int ncell3, const int *__restrict__ flags,
-                             int *__restrict__ start)
+// exclusive scan of the per-rank counts by one block
+__device__ void scan_cells(const RebuildArgs &a, int *part)
 {
-  if (!flags[kFlagRebuild])
-    return;
-  __shared__ int part[kScanThreads];
-  const int per = (ncell3 + kScanThreads - 1) / kScanThreads;
+  const int nt = blockDim.x;
+  const int per = (a.ncell3 + nt - 1) / nt;
   const int beg = threadIdx.x * per;
-  const int end = min(beg + per, ncell3);
+  const int end = min(beg + per, a.ncell3);
   int s = 0;
   for (int i = beg; i < end; i++)
-    s += count[i];
+    s += a.cell_count[i];
   part[threadIdx.x] = s;
   __syncthreads();
   // Hillis-Steele inclusive scan of the partial sums
-  for (int off = 1; off < kScanThreads; off <<= 1) {
+  for (int off = 1; off < nt; off <<= 1) {
     const int v = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
     __syncthreads();
     part[threadIdx.x] += v;
@@ -177,84 +189,40 @@ __global__ void k_scan_cells(const int *__restrict__ count, int ncell3, const in
   }
   int run = threadIdx.x > 0 ? part[threadIdx.x - 1] : 0;
   for (int i = beg; i < end; i++) {
-    start[i] = run;
-    run += count[i];
+    a.start[i] = run;
+    run += a.cell_count[i];
   }
-  if (threadIdx.x == kScanThreads - 1)
-    start[ncell3] = part[kScanThreads - 1];
+  if (threadIdx.x == nt - 1)
+    a.start[a.ncell3] = part[nt - 1];
 }
 
-__global__ void k_cell_scatter(int ngroup, const int *__restrict__ cell_of_group,
-                               const int *__restrict__ cell_rank, const int *__restrict__ start,
-                               const int *__restrict__ slot, const int *__restrict__ flags,
-                               int *__restrict__ sorted)
-{
-  if (!flags[kFlagRebuild])
-    return;
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= ngroup)
-    return;
-  sorted[start[cell_rank[cell_of_group[g]]] + slot[g]] = g;
-}
-
-// order each cell's members by group index (deterministic lists), then record
+// order a cell's members by group index (deterministic lists), then record
 // sorted positions and the anchors the list is built from
-__global__ void k_cell_finish(int ncell3, const int *__restrict__ start, const double *__restrict__ last,
-                              const int *__restrict__ flags, int *__restrict__ sorted,
-                              int *__restrict__ rank, double *__restrict__ anchor_sorted)
+__device__ __forceinline__ void cell_finish(const RebuildArgs &a, int c)
 {
-  if (!flags[kFlagRebuild])
-    return;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncell3)
-    return;
-  const int b = start[c], e = start[c + 1];
+  const int b = a.start[c], e = a.start[c + 1];
   for (int i = b + 1; i < e; i++) {
-    const int v = sorted[i];
+    const int v = a.sorted[i];
     int j = i - 1;
-    while (j >= b && sorted[j] > v) {
-      sorted[j + 1] = sorted[j];
+    while (j >= b && a.sorted[j] > v) {
+      a.sorted[j + 1] = a.sorted[j];
       j--;
     }
-    sorted[j + 1] = v;
+    a.sorted[j + 1] = v;
   }
   for (int i = b; i < e; i++) {
-    const int g = sorted[i];
-    rank[g] = i;
-    anchor_sorted[3 * i] = last[3 * g];
-    anchor_sorted[3 * i + 1] = last[3 * g + 1];
-    anchor_sorted[3 * i + 2] = last[3 * g + 2];
+    const int g = a.sorted[i];
+    a.rank[g] = i;
+    a.anchor_sorted[3 * i] = a.last[3 * g];
+    a.anchor_sorted[3 * i + 1] = a.last[3 * g + 1];
+    a.anchor_sorted[3 * i + 2] = a.last[3 * g + 2];
   }
 }
-
-struct BuildArgs {
-  int ngroup, nstencil, rowcap;
-  CellGeom cg;
-  Box box;
-  const int *stencil;        // 3 per offset, components in [0, n)
-  const int *sorted;
-  const int *cell_of_group;
-  const int *cell_rank;
-  const int *start;
-  const double *anchor_sorted;
-  const int *flags;
-  int *nbr;
-  int *nbr_count;
-  int *flags_w;
-};
-
-constexpr int kBuildWarps = 8;
 
 // one warp per sorted group; lanes walk stencil cells, members are compacted
 // into the row with a ballot
-__global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(BuildArgs a)
+__device__ __forceinline__ void build_row(const RebuildArgs &a, int p, int lane)
 {
-  if (!a.flags[kFlagRebuild])
-    return;
-  const int lane = threadIdx.x & 31;
-  const int p = blockIdx.x * kBuildWarps + (threadIdx.x >> 5);
-  if (p >= a.ngroup)
-    return;
   const int n = a.cg.n;
   const int gi = a.sorted[p];
   const int ci = a.cell_of_group[gi];
@@ -303,60 +271,87 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(BuildArgs a)
   if (lane == 0) {
     a.nbr_count[p] = min(count, a.rowcap);
     if (count > a.rowcap)
-      atomicMax(&a.flags_w[kFlagOverflow], count);
-    atomicMax(&a.flags_w[kFlagMaxRow], count);
+      atomicMax(&a.flags[kFlagOverflow], count);
+    atomicMax(&a.flags[kFlagMaxRow], count);
   }
 }
 
-cudaError_t launch_gather_anchors(mmnb_handle *h, const double *d_r)
+// The whole rebuild in one cooperative launch: cell assignment, counting-sort
+// scan, scatter, per-cell ordering, list rows, separated by grid-wide
+// barriers.  Without a rebuild due every block returns at once (the decision
+// is read from device memory, so the launch sits in a CUDA graph unchanged).
+__global__ void __launch_bounds__(kRebuildThreads) k_list_rebuild(RebuildArgs a)
 {
-  k_gather_anchors<<<div_up(h->ngroup, 256), 256, 0, h->stream>>>(d_r, h->d_group, h->ngroup, h->d_anchor);
+  if (!a.flags[kFlagRebuild])
+    return;
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  __shared__ int part[kRebuildThreads];
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  for (int g = tid; g < a.ngroup; g += nth)
+    cell_assign(a, g);
+  grid.sync();
+  if (blockIdx.x == 0)
+    scan_cells(a, part);
+  grid.sync();
+  for (int g = tid; g < a.ngroup; g += nth)
+    a.sorted[a.start[a.cell_rank[a.cell_of_group[g]]] + a.slot[g]] = g;
+  grid.sync();
+  for (int c = tid; c < a.ncell3; c += nth)
+    cell_finish(a, c);
+  grid.sync();
+  const int lane = threadIdx.x & 31;
+  for (int p = tid >> 5; p < a.ngroup; p += nth >> 5)
+    build_row(a, p, lane);
+}
+
+cudaError_t launch_list_check(mmnb_handle *h, const double *d_r, int force)
+{
+  k_list_check<<<h->top2_blocks, kCheckThreads, 0, h->stream>>>(
+      d_r, h->d_group, h->ngroup, h->d_last, h->nlw, h->first ? 1 : 0, force, h->cfg.rebuild_interval, h->d_anchor,
+      h->d_top2, h->d_flags, h->d_cell_count, h->ncell3);
   h->launches += 1;
   return cudaGetLastError();
 }
 
-cudaError_t launch_rebuild_decide(mmnb_handle *h, int force)
+cudaError_t launch_list_rebuild(mmnb_handle *h)
 {
-  k_top2<<<h->top2_blocks, kTop2Threads, 0, h->stream>>>(h->d_anchor, h->d_last, h->ngroup, h->d_top2);
-  k_decide<<<1, kTop2Threads, 0, h->stream>>>(h->d_top2, h->top2_blocks, h->nlw, h->first ? 1 : 0, force,
-                                               h->cfg.rebuild_interval, h->d_flags);
-  h->launches += 2;
-  return cudaGetLastError();
-}
-
-cudaError_t launch_build_list(mmnb_handle *h)
-{
-  cudaError_t e;
-  if ((e = cudaMemsetAsync(h->d_cell_count, 0, sizeof(int) * h->ncell3, h->stream)) != cudaSuccess)
-    return e;
-  k_cell_assign<<<div_up(h->ngroup, 256), 256, 0, h->stream>>>(h->d_anchor, h->ngroup, h->cg, h->d_cell_rank,
-                                                                h->d_flags, h->d_cell_of_group, h->d_cell_count,
-                                                                h->d_slot, h->d_last);
-  k_scan_cells<<<1, kScanThreads, 0, h->stream>>>(h->d_cell_count, h->ncell3, h->d_flags, h->d_cell_start);
-  k_cell_scatter<<<div_up(h->ngroup, 256), 256, 0, h->stream>>>(h->ngroup, h->d_cell_of_group, h->d_cell_rank,
-                                                                 h->d_cell_start, h->d_slot, h->d_flags,
-                                                                 h->d_sorted);
-  k_cell_finish<<<div_up(h->ncell3, 128), 128, 0, h->stream>>>(h->ncell3, h->d_cell_start, h->d_last, h->d_flags,
-                                                                h->d_sorted, h->d_rank, h->d_anchor_sorted);
-  BuildArgs a;
+  if (h->rebuild_grid == 0) {
+    int per_sm = 0, nsm = 0;
+    cudaError_t e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_list_rebuild, kRebuildThreads, 0)) !=
+            cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->dev)) != cudaSuccess)
+      return e;
+    if (per_sm < 1)
+      return cudaErrorLaunchOutOfResources;
+    h->rebuild_grid = std::min(per_sm * nsm, div_up(h->ngroup, kBuildWarps));
+  }
+  RebuildArgs a;
   a.ngroup = h->ngroup;
+  a.ncell3 = h->ncell3;
   a.nstencil = h->nstencil;
   a.rowcap = h->rowcap;
   a.cg = h->cg;
   a.box = h->box;
-  a.stencil = h->d_stencil;
-  a.sorted = h->d_sorted;
-  a.cell_of_group = h->d_cell_of_group;
+  a.anchor = h->d_anchor;
   a.cell_rank = h->d_cell_rank;
-  a.start = h->d_cell_start;
-  a.anchor_sorted = h->d_anchor_sorted;
+  a.stencil = h->d_stencil;
   a.flags = h->d_flags;
+  a.cell_of_group = h->d_cell_of_group;
+  a.cell_count = h->d_cell_count;
+  a.slot = h->d_slot;
+  a.start = h->d_cell_start;
+  a.sorted = h->d_sorted;
+  a.rank = h->d_rank;
+  a.last = h->d_last;
+  a.anchor_sorted = h->d_anchor_sorted;
   a.nbr = h->d_nbr;
   a.nbr_count = h->d_nbr_count;
-  a.flags_w = h->d_flags;
-  k_build_list<<<div_up(h->ngroup, kBuildWarps), kBuildWarps * 32, 0, h->stream>>>(a);
-  h->launches += 5;
-  return cudaGetLastError();
+  void *args[] = {&a};
+  h->launches += 1;
+  return cudaLaunchCooperativeKernel((const void *) k_list_rebuild, dim3(h->rebuild_grid), dim3(kRebuildThreads),
+                                     args, 0, h->stream);
 }
 
 }  // namespace mmnb
