@@ -228,6 +228,33 @@ int mmnb_kspace_field_noalloc(int nsite, const double *d_r, const double *d_q, i
                               const double box[3], double eta, double kspace_cutoff,
                               double *d_phi, double *d_evec, void *stream);
 
+/* ---- molecular dynamics on the device ------------------------------------
+   Velocity Verlet with rigid 3-site water, replacing the MD loop of
+   MDyn::run (src/mdyn.cpp:142-160: half kick, drift, constrain positions,
+   forces, half kick, constrain velocities) and the ConstraintGroup
+   SHAKE/RATTLE solves it calls (src/constraint.cpp:295-358), whose converged
+   results SETTLE (positions) and a 3 x 3 velocity solve give in closed form.
+   Units as the reference's: A, ps, kcal/mol, masses in g/mol / 418.4
+   (include/units.h:161-168).  One step is a CUDA graph on the handle's
+   stream (forces from mmnb_compute_device of h). */
+typedef struct mmnb_md mmnb_md;
+
+/* site_mass: nsite masses (reference mass units).  rigid_water: every group
+   is [O, H, H] (sites 3g..3g+2) constrained to O-H = r_oh and H-O-H =
+   hoh_angle_deg; 0 integrates without constraints.  dt in ps. */
+int mmnb_md_create(mmnb_handle *h, const double *site_mass, double dt, int rigid_water, double r_oh,
+                   double hoh_angle_deg, mmnb_md **out);
+/* Host positions and velocities (3*nsite each; v may be NULL for zero).
+   Velocities are projected onto the constraints and the forces evaluated. */
+int mmnb_md_set_state(mmnb_md *md, const double *r, const double *v);
+/* nsteps steps; energies (3*nsteps: kinetic, potential, conserved per step)
+   may be NULL.  MMNB_ERR_OVERFLOW when a neighbour row outgrew its capacity
+   during the run. */
+int mmnb_md_run(mmnb_md *md, int nsteps, double *energies);
+int mmnb_md_get_state(mmnb_md *md, double *r, double *v);
+const char *mmnb_md_last_error(const mmnb_md *md);
+int mmnb_md_destroy(mmnb_md *md);
+
 #ifdef __cplusplus
 }
 #endif
