@@ -228,6 +228,22 @@ int mmnb_kspace_field_noalloc(int nsite, const double *d_r, const double *d_q, i
                               const double box[3], double eta, double kspace_cutoff,
                               double *d_phi, double *d_evec, void *stream);
 
+/* ---- adjoint --------------------------------------------------------------
+   Gradients of one evaluation with respect to uniform scales of all charges,
+   all LJ sigmas and all LJ epsilons (each at 1), for the force-field fits the
+   reference runs through WeakCouple::update and BCIFit (src/msimprog.cpp:855-876,
+   src/bcifit.cpp:44-123) on the per-type parameters ElecLJ::types_changed maps
+   to sites (src/eleclj.cpp:440-503).  For rigid water with q_H = -q_O/2 and LJ
+   on O only, gradient / parameter value gives d/d(q_O, sigma_O, epsilon_O).
+   Runs the forward evaluation at r (f and u ADDED when non-NULL), then a
+   backward kernel that recomputes the LJ pair terms in FP64.
+   grad_u[3]: dU/d(scales).  dl_df (3*nsite, may be NULL) is dL/dF of a loss of
+   the forces; grad_l[3] (may be NULL) receives sum_i dl_df_i . dF_i/d(scales).
+   MMNB_ERR_UNSUPPORTED unless every LJ site is its group's anchor and there
+   are no group exclusions or 1-4 pairs. */
+int mmnb_backward(mmnb_handle *h, const double *r, const double *dl_df, double *f, double *u,
+                  double grad_u[3], double grad_l[3]);
+
 /* ---- molecular dynamics on the device ------------------------------------
    Velocity Verlet with rigid 3-site water, replacing the MD loop of
    MDyn::run (src/mdyn.cpp:142-160: half kick, drift, constrain positions,

@@ -375,7 +375,7 @@ void free_all(mmnb_handle *h)
                   h->d_phi, h->d_evec, h->d_ljf, h->d_lj_part, h->d_elec_part, h->d_energy, h->d_r, h->d_f,
                   h->d_mesh, h->d_meshk, h->d_green, h->d_kvec, h->d_egrid, h->d_egridk, h->d_mesh32,
                   h->d_meshk32, h->d_green32, h->d_mesh_fx, h->d_kint, h->d_kvecs, h->d_ak, h->d_skc,
-                  h->mx.site, h->mx.par, h->mx.anchor, h->mx.lj, h->mx.acc, h->d_wsum};
+                  h->mx.site, h->mx.par, h->mx.anchor, h->mx.lj, h->mx.acc, h->d_wsum, h->d_bwd};
   for (void *p : ptrs)
     if (p)
       cudaFree(p);
@@ -435,6 +435,22 @@ void timing_mark(mmnb_handle *h, const char *name)
   cudaEventRecord(t.pool[t.used], h->stream);
   t.names.push_back(name);
   t.used++;
+}
+
+// The reference's LJ tail (src/eleclj.cpp:1247-1266) for totals A and B.
+double lj_tail_ab(const mmnb_handle *h, double A, double B)
+{
+  const double rhi = h->rc, rlo = rhi - h->cfg.smoothing_width;
+  const double rlo2 = rlo * rlo, rlo3 = rlo2 * rlo, rlo4 = rlo3 * rlo;
+  const double rlo5 = rlo4 * rlo, rlo6 = rlo5 * rlo, rlo7 = rlo6 * rlo, rlo9 = rlo7 * rlo2;
+  const double rhi2 = rhi * rhi, rhi3 = rhi2 * rhi, rhi4 = rhi3 * rhi, rhi5 = rhi4 * rhi;
+  const double rhi6 = rhi5 * rhi, rhi7 = rhi6 * rhi;
+  return 2 * M_PI / h->volume *
+         (A / (9 * rlo9) + B / (3 * rlo3) -
+          (rhi - rlo) / (63 * rhi3 * rlo9 * pow(rhi + rlo, 5)) *
+              (3 * B * rhi3 * rlo6 * (7 * rhi4 + 42 * rhi3 * rlo + 112 * rhi2 * rlo2 + 150 * rhi * rlo3 + 25 * rlo4) +
+               A * (7 * rhi7 + 42 * rhi6 * rlo + 112 * rhi5 * rlo2 + 182 * rhi4 * rlo3 + 217 * rhi3 * rlo4 +
+                    224 * rhi2 * rlo5 + 192 * rhi * rlo6 + 32 * rlo7)));
 }
 
 }  // namespace mmnb
@@ -668,22 +684,7 @@ int mmnb_create(const mmnb_config *c, int nsite, int ngroup, const int *group, i
   return MMNB_OK;
 }
 
-// The reference's LJ tail (src/eleclj.cpp:1247-1266).
-static double lj_tail(const mmnb_handle *h)
-{
-  const double rhi = h->rc, rlo = rhi - h->cfg.smoothing_width;
-  const double A = h->totA, B = h->totB;
-  const double rlo2 = rlo * rlo, rlo3 = rlo2 * rlo, rlo4 = rlo3 * rlo;
-  const double rlo5 = rlo4 * rlo, rlo6 = rlo5 * rlo, rlo7 = rlo6 * rlo, rlo9 = rlo7 * rlo2;
-  const double rhi2 = rhi * rhi, rhi3 = rhi2 * rhi, rhi4 = rhi3 * rhi, rhi5 = rhi4 * rhi;
-  const double rhi6 = rhi5 * rhi, rhi7 = rhi6 * rhi;
-  return 2 * M_PI / h->volume *
-         (A / (9 * rlo9) + B / (3 * rlo3) -
-          (rhi - rlo) / (63 * rhi3 * rlo9 * pow(rhi + rlo, 5)) *
-              (3 * B * rhi3 * rlo6 * (7 * rhi4 + 42 * rhi3 * rlo + 112 * rhi2 * rlo2 + 150 * rhi * rlo3 + 25 * rlo4) +
-               A * (7 * rhi7 + 42 * rhi6 * rlo + 112 * rhi5 * rlo2 + 182 * rhi4 * rlo3 + 217 * rhi3 * rlo4 +
-                    224 * rhi2 * rlo5 + 192 * rhi * rlo6 + 32 * rlo7)));
-}
+static double lj_tail(const mmnb_handle *h) { return lj_tail_ab(h, h->totA, h->totB); }
 
 static void update_energy_constants(mmnb_handle *h, double qsum)
 {

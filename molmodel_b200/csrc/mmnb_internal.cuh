@@ -147,6 +147,8 @@ struct mmnb_handle {
   // [0], [1]: fixed-point Coulomb and LJ pair energies of the water kernel;
   // [2]: block counter of the finalize kernel's last-block reduction
   unsigned long long *d_wsum = nullptr;
+  double *d_bwd = nullptr;           // backward pass: row partials and dL/dF (allocated on first use)
+  size_t bwd_cap = 0;
   int lj_pair_blocks = 0, lj_excl_blocks = 0;
   double *d_elec_part = nullptr;     // per block
   int elec_blocks = 0;
@@ -195,6 +197,8 @@ struct mmnb_handle {
 namespace mmnb {
 
 // ---- launchers (defined in the .cu files) ----------------------------------
+// LJ tail correction (src/eleclj.cpp:1247-1266) for totals A and B; linear in both
+double lj_tail_ab(const mmnb_handle *h, double A, double B);
 // anchors, rebuild decision; then the rebuild (a no-op launch when not due)
 cudaError_t launch_list_check(mmnb_handle *h, const double *d_r, int force);
 cudaError_t launch_list_rebuild(mmnb_handle *h);
