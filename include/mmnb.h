@@ -270,6 +270,23 @@ int mmnb_md_run(mmnb_md *md, int nsteps, double *energies);
 int mmnb_md_get_state(mmnb_md *md, double *r, double *v);
 const char *mmnb_md_last_error(const mmnb_md *md);
 int mmnb_md_destroy(mmnb_md *md);
+/* Multiply the velocities by factor (a temperature swap of replica exchange
+   rescales them by sqrt(T_new / T_old)). */
+int mmnb_md_scale_velocities(mmnb_md *md, double factor);
+
+/* Replica batch: n integrators (each on its own handle and stream, after
+   mmnb_md_set_state) advanced together, one CUDA graph launch per step with
+   an independent branch per replica, so replicas of uneven size share the
+   GPU.  Replaces the one-process-per-replica layout of MDyn's replica
+   exchange (src/mdyn.cpp:317-351, one MPI rank per replica); the exchange
+   itself (energies from the logs, temperature swaps) is the caller's.
+   energies: n host arrays of 3*nsteps (kinetic, potential, conserved per
+   step), or NULL; any entry may be NULL. */
+typedef struct mmnb_md_batch mmnb_md_batch;
+int mmnb_md_batch_create(mmnb_md *const *mds, int n, mmnb_md_batch **out);
+int mmnb_md_batch_run(mmnb_md_batch *b, int nsteps, double *const *energies);
+const char *mmnb_md_batch_last_error(const mmnb_md_batch *b);
+int mmnb_md_batch_destroy(mmnb_md_batch *b);
 
 #ifdef __cplusplus
 }

@@ -89,6 +89,11 @@ SIGNATURES = [
     ("mmnb_md_get_state", ctypes.c_int, [_vp, _dp, _dp]),
     ("mmnb_md_last_error", ctypes.c_char_p, [_vp]),
     ("mmnb_md_destroy", ctypes.c_int, [_vp]),
+    ("mmnb_md_scale_velocities", ctypes.c_int, [_vp, ctypes.c_double]),
+    ("mmnb_md_batch_create", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp)]),
+    ("mmnb_md_batch_run", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_dp)]),
+    ("mmnb_md_batch_last_error", ctypes.c_char_p, [_vp]),
+    ("mmnb_md_batch_destroy", ctypes.c_int, [_vp]),
 ]
 
 _lib = None

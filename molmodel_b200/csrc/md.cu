@@ -19,6 +19,8 @@
 // the last block, and each step's (kinetic, potential, conserved) energies are
 // appended to a device log that is read back once per run.
 
+#include <algorithm>
+#include <string>
 #include <vector>
 
 #include "mmnb_internal.cuh"
@@ -43,9 +45,28 @@ struct mmnb_md {
   std::string err;
 };
 
+// Several replicas stepped by one graph launch: an independent branch per
+// replica, each on its replica's stream.
+struct mmnb_md_batch {
+  std::vector<mmnb_md *> md;
+  cudaStream_t master = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> done;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::string err;
+};
+
 namespace mmnb {
 
 constexpr int kMdThreads = 256;
+
+__global__ void k_md_scale(double *__restrict__ v, int n, double s)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n)
+    v[i] *= s;
+}
 
 struct MdArgs {
   int nsite, nmol, rigid;
@@ -386,9 +407,28 @@ int mmnb_md_set_state(mmnb_md *md, const double *r, const double *v)
   return MMNB_OK;
 }
 
-static int md_capture(mmnb_md *md, double *log)
+// Record one step on the handle's stream (which must be capturing).
+static int md_record(mmnb_md *md, double *log)
 {
   mmnb_handle *h = md->h;
+  const MdArgs a = md_args(md, log);
+  const int n = md->rigid ? md->nmol : md->nsite;
+  k_md_drift<<<div_up(n, 128), 128, 0, h->stream>>>(a);
+  cudaError_t e = cudaMemsetAsync(md->d_f, 0, 3 * (size_t) md->nsite * sizeof(double), h->stream);
+  if (e != cudaSuccess)
+    return md_fail(md, MMNB_ERR_CUDA, cudaGetErrorString(e));
+  const int s = mmnb_compute_device(h, md->d_r, md->d_f, md->d_energy);
+  if (s)
+    return md_fail(md, s, mmnb_last_error(h));
+  k_md_kick<<<md->ke_blocks, kMdThreads, 0, h->stream>>>(a, 1);
+  e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return md_fail(md, MMNB_ERR_CUDA, cudaGetErrorString(e));
+  return MMNB_OK;
+}
+
+static void md_drop_graph(mmnb_md *md)
+{
   if (md->exec) {
     cudaGraphExecDestroy(md->exec);
     md->exec = nullptr;
@@ -397,24 +437,41 @@ static int md_capture(mmnb_md *md, double *log)
     cudaGraphDestroy(md->graph);
     md->graph = nullptr;
   }
-  const MdArgs a = md_args(md, log);
-  const int n = md->rigid ? md->nmol : md->nsite;
+}
+
+static int md_capture(mmnb_md *md, double *log)
+{
+  mmnb_handle *h = md->h;
+  md_drop_graph(md);
   MDCK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   h->capturing = true;
-  k_md_drift<<<div_up(n, 128), 128, 0, h->stream>>>(a);
-  cudaError_t e = cudaMemsetAsync(md->d_f, 0, 3 * (size_t) md->nsite * sizeof(double), h->stream);
-  int s = e == cudaSuccess ? mmnb_compute_device(h, md->d_r, md->d_f, md->d_energy) : MMNB_ERR_CUDA;
-  if (s == MMNB_OK)
-    k_md_kick<<<md->ke_blocks, kMdThreads, 0, h->stream>>>(a, 1);
+  const int s = md_record(md, log);
   cudaGraph_t g = nullptr;
   const cudaError_t ec = cudaStreamEndCapture(h->stream, &g);
   h->capturing = false;
-  if (s)
-    return md_fail(md, s, mmnb_last_error(h));
-  MDCK(e);
+  if (s) {
+    if (g)
+      cudaGraphDestroy(g);
+    return s;
+  }
   MDCK(ec);
   md->graph = g;
   MDCK(cudaGraphInstantiate(&md->exec, g, 0));
+  return MMNB_OK;
+}
+
+// the log holds at least nsteps steps (a reallocation invalidates the graph)
+static int md_reserve_log(mmnb_md *md, int nsteps)
+{
+  if (md->log_cap >= nsteps)
+    return MMNB_OK;
+  if (md->d_log)
+    cudaFree(md->d_log);
+  md->d_log = nullptr;
+  md->log_cap = 0;
+  MDCK(cudaMalloc(&md->d_log, 3 * (size_t) nsteps * sizeof(double)));
+  md->log_cap = nsteps;
+  md_drop_graph(md);
   return MMNB_OK;
 }
 
@@ -425,18 +482,8 @@ int mmnb_md_run(mmnb_md *md, int nsteps, double *energies)
   mmnb_handle *h = md->h;
   if (nsteps == 0)
     return MMNB_OK;
-  if (md->log_cap < nsteps) {
-    if (md->d_log)
-      cudaFree(md->d_log);
-    md->d_log = nullptr;
-    md->log_cap = 0;
-    MDCK(cudaMalloc(&md->d_log, 3 * (size_t) nsteps * sizeof(double)));
-    md->log_cap = nsteps;
-    if (md->exec) {
-      cudaGraphExecDestroy(md->exec);
-      md->exec = nullptr;
-    }
-  }
+  if (const int s = md_reserve_log(md, nsteps))
+    return s;
   if (!md->exec) {
     const int s = md_capture(md, md->d_log);
     if (s)
@@ -492,6 +539,175 @@ int mmnb_md_destroy(mmnb_md *md)
     if (q)
       cudaFree(q);
   delete md;
+  return MMNB_OK;
+}
+
+int mmnb_md_scale_velocities(mmnb_md *md, double factor)
+{
+  if (!md)
+    return MMNB_ERR_ARG;
+  mmnb_handle *h = md->h;
+  const int n3 = 3 * md->nsite;
+  k_md_scale<<<div_up(n3, 256), 256, 0, h->stream>>>(md->d_v, n3, factor);
+  MDCK(cudaGetLastError());
+  MDCK(cudaStreamSynchronize(h->stream));
+  return MMNB_OK;
+}
+
+// ---- replica batch --------------------------------------------------------------
+
+int mmnb_md_batch_create(mmnb_md *const *mds, int n, mmnb_md_batch **out)
+{
+  if (!out || !mds || n <= 0)
+    return MMNB_ERR_ARG;
+  *out = nullptr;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < i; j++)
+      if (!mds[i] || mds[i] == mds[j] || mds[i]->h == mds[j]->h || mds[i]->h->stream == mds[j]->h->stream)
+        return MMNB_ERR_ARG;  // every replica needs its own handle and stream
+  mmnb_md_batch *b = new mmnb_md_batch;
+  b->md.assign(mds, mds + n);
+  if (cudaSetDevice(mds[0]->h->dev) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->master, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) {
+    mmnb_md_batch_destroy(b);
+    return MMNB_ERR_CUDA;
+  }
+  b->done.resize(n, nullptr);
+  for (int i = 0; i < n; i++)
+    if (cudaEventCreateWithFlags(&b->done[i], cudaEventDisableTiming) != cudaSuccess) {
+      mmnb_md_batch_destroy(b);
+      return MMNB_ERR_CUDA;
+    }
+  *out = b;
+  return MMNB_OK;
+}
+
+static int batch_fail(mmnb_md_batch *b, int code, const std::string &msg)
+{
+  b->err = msg;
+  return code;
+}
+
+// one graph: a fork from the master stream into every replica's stream, each
+// replica's step recorded on its own stream, a join back
+static int batch_capture(mmnb_md_batch *b)
+{
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  if (b->graph) {
+    cudaGraphDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  cudaError_t e = cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess)
+    return batch_fail(b, MMNB_ERR_CUDA, cudaGetErrorString(e));
+  int s = MMNB_OK;
+  e = cudaEventRecord(b->fork, b->master);
+  for (size_t i = 0; i < b->md.size() && e == cudaSuccess && !s; i++) {
+    mmnb_md *md = b->md[i];
+    mmnb_handle *h = md->h;
+    e = cudaStreamWaitEvent(h->stream, b->fork, 0);
+    if (e != cudaSuccess)
+      break;
+    h->capturing = true;
+    s = md_record(md, md->d_log);
+    h->capturing = false;
+    if (s)
+      break;
+    if ((e = cudaEventRecord(b->done[i], h->stream)) == cudaSuccess)
+      e = cudaStreamWaitEvent(b->master, b->done[i], 0);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(b->master, &g);
+  if (s || e != cudaSuccess || ec != cudaSuccess) {
+    if (g)
+      cudaGraphDestroy(g);
+    if (s)
+      return batch_fail(b, s, "replica step: " + b->md[0]->err);
+    return batch_fail(b, MMNB_ERR_CUDA, cudaGetErrorString(e != cudaSuccess ? e : ec));
+  }
+  b->graph = g;
+  e = cudaGraphInstantiate(&b->exec, g, 0);
+  if (e != cudaSuccess)
+    return batch_fail(b, MMNB_ERR_CUDA, cudaGetErrorString(e));
+  return MMNB_OK;
+}
+
+int mmnb_md_batch_run(mmnb_md_batch *b, int nsteps, double *const *energies)
+{
+  if (!b || nsteps < 0)
+    return MMNB_ERR_ARG;
+  if (nsteps == 0)
+    return MMNB_OK;
+  for (mmnb_md *md : b->md) {
+    const int cap = md->log_cap;
+    if (const int s = md_reserve_log(md, nsteps))
+      return batch_fail(b, s, md->err);
+    if (md->log_cap != cap && b->exec) {
+      cudaGraphExecDestroy(b->exec);
+      b->exec = nullptr;
+    }
+  }
+  if (!b->exec)
+    if (const int s = batch_capture(b))
+      return s;
+  cudaError_t e = cudaSuccess;
+  for (mmnb_md *md : b->md) {
+    if (e == cudaSuccess)
+      e = cudaMemsetAsync(md->d_ctl + 1, 0, sizeof(unsigned long long), md->h->stream);
+    if (e == cudaSuccess)
+      e = cudaMemsetAsync(md->h->d_flags + kFlagOverflow, 0, sizeof(int), md->h->stream);
+    if (e == cudaSuccess)
+      e = cudaEventRecord(md->h->ev_fork, md->h->stream);
+    if (e == cudaSuccess)
+      e = cudaStreamWaitEvent(b->master, md->h->ev_fork, 0);
+  }
+  for (int i = 0; i < nsteps && e == cudaSuccess; i++)
+    e = cudaGraphLaunch(b->exec, b->master);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(b->master);
+  if (e != cudaSuccess)
+    return batch_fail(b, MMNB_ERR_CUDA, cudaGetErrorString(e));
+  int overflow = 0;
+  for (size_t i = 0; i < b->md.size(); i++) {
+    mmnb_md *md = b->md[i];
+    int flags[kFlagCount];
+    e = cudaMemcpy(flags, md->h->d_flags, sizeof(flags), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && energies && energies[i])
+      e = cudaMemcpy(energies[i], md->d_log, 3 * (size_t) nsteps * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+      return batch_fail(b, MMNB_ERR_CUDA, cudaGetErrorString(e));
+    md->h->evals += nsteps;
+    overflow = std::max(overflow, flags[kFlagOverflow]);
+  }
+  if (overflow > 0)
+    return batch_fail(b, MMNB_ERR_OVERFLOW, "a replica's neighbour row outgrew its capacity during the run");
+  return MMNB_OK;
+}
+
+const char *mmnb_md_batch_last_error(const mmnb_md_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+int mmnb_md_batch_destroy(mmnb_md_batch *b)
+{
+  if (!b)
+    return MMNB_OK;
+  if (b->master)
+    cudaStreamSynchronize(b->master);
+  if (b->exec)
+    cudaGraphExecDestroy(b->exec);
+  if (b->graph)
+    cudaGraphDestroy(b->graph);
+  for (cudaEvent_t ev : b->done)
+    if (ev)
+      cudaEventDestroy(ev);
+  if (b->fork)
+    cudaEventDestroy(b->fork);
+  if (b->master)
+    cudaStreamDestroy(b->master);
+  delete b;
   return MMNB_OK;
 }
 

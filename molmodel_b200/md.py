@@ -64,10 +64,49 @@ class MDyn:
         self._check(load().mmnb_md_get_state(self._md, _d(r), _d(v)))
         return r, v
 
+    def scale_velocities(self, factor):
+        self._check(load().mmnb_md_scale_velocities(self._md, float(factor)))
+
     def close(self):
         if getattr(self, "_md", None):
             load().mmnb_md_destroy(self._md)
             self._md = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ReplicaBatch:
+    """Several MDyn integrators (each with its own potential handle) advanced
+    together: one CUDA graph launch per step with a branch per replica."""
+
+    def __init__(self, mds):
+        lib = load()
+        self.mds = list(mds)
+        arr = (ctypes.c_void_p * len(self.mds))(*[m._md.value for m in self.mds])
+        h = ctypes.c_void_p()
+        st = lib.mmnb_md_batch_create(arr, len(self.mds), ctypes.byref(h))
+        if st:
+            raise MmnbError(st, "mmnb_md_batch_create: " + lib.mmnb_status_string(st).decode())
+        self._b = h
+
+    def run(self, steps):
+        """Advance every replica `steps` steps; returns a list of (steps, 3)
+        energy arrays (kinetic, potential, conserved)."""
+        out = [np.zeros((steps, 3)) for _ in self.mds]
+        ptrs = (_dp * len(out))(*[_d(e) for e in out])
+        st = load().mmnb_md_batch_run(self._b, int(steps), ptrs)
+        if st:
+            raise MmnbError(st, load().mmnb_md_batch_last_error(self._b).decode())
+        return out
+
+    def close(self):
+        if getattr(self, "_b", None):
+            load().mmnb_md_batch_destroy(self._b)
+            self._b = None
 
     def __del__(self):
         try:

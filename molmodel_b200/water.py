@@ -155,6 +155,28 @@ def water_box(n, seed, density=0.997, q_o=Q_O_E):
                     seed=seed, charges_e=charges)
 
 
+def water_box_n(nwater, seed, density=0.997, q_o=Q_O_E):
+    """``nwater`` waters (any count) at ``density``: the first ``nwater`` sites
+    of a seeded permutation of the smallest cubic lattice that holds them,
+    with seeded random orientations."""
+    m = int(math.ceil(nwater ** (1.0 / 3.0) - 1e-9))
+    L = box_length(nwater, density)
+    pick = np.sort(np.argsort(splitmix64_uniform(seed ^ 0x9E3779B9, m ** 3))[:nwater])
+    ijk = np.stack([pick // (m * m), (pick // m) % m, pick % m], axis=1).astype(np.float64)
+    centres = (ijk + 0.5) * (L / m)
+    u = splitmix64_uniform(seed, 3 * nwater).reshape(nwater, 3)
+    R = _rotations(u)
+    half = math.radians(THETA_HOH) / 2
+    body = np.array([[0.0, 0.0, 0.0],
+                     [R_OH * math.sin(half), 0.0, R_OH * math.cos(half)],
+                     [-R_OH * math.sin(half), 0.0, R_OH * math.cos(half)]])
+    pos = centres[:, None, :] + np.einsum("nij,sj->nsi", R, body)
+    masses = np.tile([MASS_O, MASS_H, MASS_H], nwater)
+    charges = np.tile([q_o, -q_o / 2, -q_o / 2], nwater)
+    return WaterBox(nwater=nwater, box=L, positions=pos.reshape(-1, 3).copy(), masses=masses,
+                    seed=seed, charges_e=charges)
+
+
 def maxwell_boltzmann(wb, temperature, seed):
     """Seeded Maxwell-Boltzmann velocities (A/ps) with zero total momentum.
 
