@@ -255,6 +255,7 @@ int setup_cells(mmnb_handle *h)
 
 int alloc_rows(mmnb_handle *h, int cap)
 {
+  drop_host_graph(h);
   h->rowcap = std::max(1, std::min(cap, h->ngroup));
   return dalloc(h, &h->d_nbr, (size_t) h->ngroup * h->rowcap);
 }
@@ -367,6 +368,16 @@ int setup_p3m(mmnb_handle *h)
 
 void free_all(mmnb_handle *h)
 {
+  drop_host_graph(h);
+  for (cudaEvent_t &ev : h->ev_chunk)
+    if (ev) {
+      cudaEventDestroy(ev);
+      ev = nullptr;
+    }
+  if (h->ev_flags) {
+    cudaEventDestroy(h->ev_flags);
+    h->ev_flags = nullptr;
+  }
   void *ptrs[] = {h->d_group, h->d_excl_ptr, h->d_excl_idx, h->d_p14_ptr, h->d_p14_idx, h->d_gexcl_ptr,
                   h->d_gexcl_idx, h->d_mask, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_cheb,
                   h->d_stencil, h->d_cell_rank, h->d_cell_of_rank, h->d_cell_of_group, h->d_cell_count,
@@ -451,6 +462,16 @@ double lj_tail_ab(const mmnb_handle *h, double A, double B)
               (3 * B * rhi3 * rlo6 * (7 * rhi4 + 42 * rhi3 * rlo + 112 * rhi2 * rlo2 + 150 * rhi * rlo3 + 25 * rlo4) +
                A * (7 * rhi7 + 42 * rhi6 * rlo + 112 * rhi5 * rlo2 + 182 * rhi4 * rlo3 + 217 * rhi3 * rlo4 +
                     224 * rhi2 * rlo5 + 192 * rhi * rlo6 + 32 * rlo7)));
+}
+
+void drop_host_graph(mmnb_handle *h)
+{
+  if (h->hgraph_exec)
+    cudaGraphExecDestroy(h->hgraph_exec);
+  if (h->hgraph)
+    cudaGraphDestroy(h->hgraph);
+  h->hgraph_exec = nullptr;
+  h->hgraph = nullptr;
 }
 
 }  // namespace mmnb
@@ -697,6 +718,7 @@ int mmnb_set_params(mmnb_handle *h, const int *site_mask, const double *q, const
 {
   if (!h || !site_mask || !q || !sig || !eps)
     return fail(h, MMNB_ERR_ARG, "null parameter array");
+  drop_host_graph(h);
   const int n = h->nsite;
   std::vector<double> rs(n, 0.0);
   h->any_q = h->any_lj = h->has_rscreen = false;
@@ -904,31 +926,89 @@ int mmnb_graph_launch(mmnb_handle *h)
   return MMNB_OK;
 }
 
+// f[i] += src[i] over [b, e), split over host threads when the range is large
+static void add_forces(double *f, const double *src, size_t b, size_t e)
+{
+  const long n = (long) (e - b);
+#pragma omp parallel for schedule(static) if (n > (1 << 16))
+  for (long i = 0; i < n; i++)
+    f[b + i] += src[b + i];
+}
+
 int mmnb_compute(mmnb_handle *h, const double *r, double *f, double *u, mmnb_energy *e, double *phi, double *evec)
 {
   if (!h || !r)
     return fail(h, MMNB_ERR_ARG, "null handle or positions");
   const size_t n3 = 3 * (size_t) h->nsite;
+  if (!h->ev_flags) {
+    CK(cudaEventCreateWithFlags(&h->ev_flags, cudaEventDisableTiming));
+    for (cudaEvent_t &ev : h->ev_chunk)
+      CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  }
   for (int attempt = 0; attempt < 2; attempt++) {
     CK(cudaMemcpyAsync(h->d_r, r, sizeof(double) * n3, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemsetAsync(h->d_f, 0, sizeof(double) * n3, h->stream));
-    CK(cudaMemsetAsync(h->d_flags + kFlagOverflow, 0, sizeof(int), h->stream));
-    h->want_fields = phi || evec;
-    const int s = mmnb_compute_device(h, h->d_r, h->d_f, h->d_energy);
-    h->want_fields = false;
-    if (s)
-      return s;
-    CK(cudaMemcpyAsync(h->h_f, h->d_f, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(h->h_out, h->d_energy, sizeof(double) * 4, cudaMemcpyDeviceToHost, h->stream));
+    // after the first call, a plain evaluation replays the handle's own graph
+    // (zeroing, list check/rebuild, pair and mesh kernels, finalize)
+    const bool graph = !h->first && !(phi || evec) && !h->timing.on && !h->force_rebuild_next;
+    if (graph && !h->hgraph_exec) {
+      CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+      h->capturing = true;
+      const long ev = h->evals, ln = h->launches;
+      cudaError_t ce = cudaMemsetAsync(h->d_f, 0, sizeof(double) * n3, h->stream);
+      if (ce == cudaSuccess)
+        ce = cudaMemsetAsync(h->d_flags + kFlagOverflow, 0, sizeof(int), h->stream);
+      const int s = ce == cudaSuccess ? mmnb_compute_device(h, h->d_r, h->d_f, h->d_energy) : MMNB_ERR_CUDA;
+      h->capturing = false;
+      cudaGraph_t g = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(h->stream, &g);
+      h->evals = ev;
+      h->host_launch_per_eval = h->launches - ln;
+      h->launches = ln;
+      if (s || ec != cudaSuccess) {
+        if (g)
+          cudaGraphDestroy(g);
+        if (s)
+          return s;
+        return fail(h, MMNB_ERR_CUDA, std::string("capture of the host call: ") + cudaGetErrorString(ec));
+      }
+      h->hgraph = g;
+      CK(cudaGraphInstantiate(&h->hgraph_exec, g, 0));
+    }
+    if (graph) {
+      CK(cudaGraphLaunch(h->hgraph_exec, h->stream));
+      h->evals++;
+      h->launches += h->host_launch_per_eval;
+    } else {
+      CK(cudaMemsetAsync(h->d_f, 0, sizeof(double) * n3, h->stream));
+      CK(cudaMemsetAsync(h->d_flags + kFlagOverflow, 0, sizeof(int), h->stream));
+      h->want_fields = phi || evec;
+      const int s = mmnb_compute_device(h, h->d_r, h->d_f, h->d_energy);
+      h->want_fields = false;
+      if (s)
+        return s;
+    }
+    // flags first (a row overflow means evaluating again), then the forces in
+    // chunks, each added to f while the next one is in flight
     CK(cudaMemcpyAsync(h->h_flags, h->d_flags, sizeof(int) * kFlagCount, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->h_out, h->d_energy, sizeof(double) * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaEventRecord(h->ev_flags, h->stream));
+    const int nch = mmnb_handle::kChunks;
+    const size_t per = (n3 + nch - 1) / nch;
+    for (int c = 0; c < nch; c++) {
+      const size_t b = std::min(n3, c * per), en = std::min(n3, b + per);
+      if (en > b)
+        CK(cudaMemcpyAsync(h->h_f + b, h->d_f + b, sizeof(double) * (en - b), cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaEventRecord(h->ev_chunk[c], h->stream));
+    }
     if (phi)
       CK(cudaMemcpyAsync(phi, h->d_phi, sizeof(double) * h->nsite, cudaMemcpyDeviceToHost, h->stream));
     if (evec)
       CK(cudaMemcpyAsync(evec, h->d_evec, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaEventSynchronize(h->ev_flags));
     h->rebuilds = h->h_flags[5];
     if (h->h_flags[kFlagOverflow] > 0) {
       // a row outgrew its capacity: grow, force a rebuild, evaluate again
+      CK(cudaStreamSynchronize(h->stream));
       const int need = h->h_flags[kFlagOverflow];
       int st = alloc_rows(h, (need + need / 4 + 63) / 32 * 32);
       if (st)
@@ -937,9 +1017,13 @@ int mmnb_compute(mmnb_handle *h, const double *r, double *f, double *u, mmnb_ene
       h->evals--;
       continue;
     }
-    if (f)
-      for (size_t i = 0; i < n3; i++)
-        f[i] += h->h_f[i];
+    for (int c = 0; c < nch; c++) {
+      CK(cudaEventSynchronize(h->ev_chunk[c]));
+      const size_t b = std::min(n3, c * per), en = std::min(n3, b + per);
+      if (f && en > b)
+        add_forces(f, h->h_f, b, en);
+    }
+    CK(cudaStreamSynchronize(h->stream));
     if (u)
       *u += h->h_out[3];
     if (e) {
@@ -968,6 +1052,7 @@ int mmnb_scale(mmnb_handle *h, double s)
 {
   if (!h || !(s > 0))
     return fail(h, MMNB_ERR_ARG, "scale factor must be > 0");
+  drop_host_graph(h);
   for (int d = 0; d < 3; d++) {
     h->box.L[d] *= s;
     h->box.invL[d] = 1 / h->box.L[d];
@@ -1004,6 +1089,7 @@ int mmnb_set_stream(mmnb_handle *h, void *stream)
 {
   if (!h)
     return MMNB_ERR_ARG;
+  drop_host_graph(h);
   CK(cudaStreamSynchronize(h->stream));
   h->stream = stream ? (cudaStream_t) stream : h->own_stream;
   if (h->plan_r2c)

@@ -191,12 +191,23 @@ struct mmnb_handle {
   // one captured evaluation (mmnb_graph_capture / mmnb_graph_launch)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
+  // the host call's own graph (d_r -> d_f, d_energy), captured on first use
+  // and dropped whenever rows, parameters, box or stream change
+  cudaGraph_t hgraph = nullptr;
+  cudaGraphExec_t hgraph_exec = nullptr;
+  long host_launch_per_eval = 0;
+  // the host call copies the forces back in chunks and adds each as it lands
+  static constexpr int kChunks = 8;
+  cudaEvent_t ev_chunk[kChunks] = {};
+  cudaEvent_t ev_flags = nullptr;
   bool capturing = false;
 };
 
 namespace mmnb {
 
 // ---- launchers (defined in the .cu files) ----------------------------------
+// drop the host call's graph (called when what it captured changes)
+void drop_host_graph(mmnb_handle *h);
 // LJ tail correction (src/eleclj.cpp:1247-1266) for totals A and B; linear in both
 double lj_tail_ab(const mmnb_handle *h, double A, double B);
 // anchors, rebuild decision; then the rebuild (a no-op launch when not due)
