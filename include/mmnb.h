@@ -228,6 +228,20 @@ int mmnb_kspace_field_noalloc(int nsite, const double *d_r, const double *d_q, i
                               const double box[3], double eta, double kspace_cutoff,
                               double *d_phi, double *d_evec, void *stream);
 
+/* ---- launch tuning ---------------------------------------------------------
+   No counterpart in the reference (its path is one CPU thread).  Launch
+   choices that change no result: tuning[0] = resident blocks per SM of the
+   rigid-water pair kernel (4 or 5: its register budget), tuning[1] = threads
+   per site of the mixed P3M charge assignment (0: one, 1: one per mesh plane),
+   tuning[2] = P3M mesh work on a second stream beside the pair kernels (1) or
+   in line (0).  mmnb_autotune times each choice over `iters` graph replays of
+   an evaluation at r (host array) and keeps the fastest; small systems gain
+   most.  It evaluates at r (advancing the rebuild counters); a graph captured
+   with mmnb_graph_capture before tuning keeps the old choices. */
+int mmnb_autotune(mmnb_handle *h, const double *r, int iters);
+int mmnb_get_tuning(mmnb_handle *h, int tuning[3]);
+int mmnb_set_tuning(mmnb_handle *h, const int tuning[3]);
+
 /* ---- adjoint --------------------------------------------------------------
    Gradients of one evaluation with respect to uniform scales of all charges,
    all LJ sigmas and all LJ epsilons (each at 1), for the force-field fits the

@@ -801,10 +801,13 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
   // back before interpolation (which adds to what the pair kernels wrote).
   // With stage timing on, the join follows at once so the marks stay serial.
   const bool p3m = h->any_q && h->cfg.include_kspace && h->p3m;
+  // the side stream pays off when the pair kernels leave room beside them;
+  // mmnb_autotune may put the mesh work in line instead (tune.p3m_side = 0)
+  const bool side = p3m && h->tune.p3m_side;
   // the mixed form's FP64 site arrays (zeroed here, then the exclusion
   // corrections) do not meet the pair kernels either: they go to the side
   // stream too
-  const bool excl_side = p3m && mixed && h->cfg.include_rspace;
+  const bool excl_side = side && mixed && h->cfg.include_rspace;
   auto zero_site_arrays = [&]() -> cudaError_t {
     cudaError_t e;
     if ((e = cudaMemsetAsync(h->d_phi, 0, sizeof(double) * h->nsite, h->stream)) != cudaSuccess ||
@@ -812,7 +815,9 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
       return e;
     return cudaMemsetAsync(h->d_ljf, 0, sizeof(double) * 3 * h->nsite, h->stream);
   };
-  if (p3m) {
+  if (p3m && !side)
+    CK(mixed ? launch_p3m_mixed(h, d_r, 1) : launch_p3m_fp64(h, d_r, 1));
+  if (side) {
     cudaStream_t main = h->stream;
     CK(cudaEventRecord(h->ev_fork, main));
     CK(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
@@ -864,7 +869,7 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
       CK(cudaMemsetAsync(h->mx.acc, 0, sizeof(long long) * h->nsite * kAccStride, h->stream));
   }
   if (p3m) {
-    if (!h->timing.on)
+    if (side && !h->timing.on)
       CK(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
     CK(mixed ? launch_p3m_mixed(h, d_r, 2) : launch_p3m_fp64(h, d_r, 2));
     timing_mark(h, "kspace");
@@ -1284,6 +1289,122 @@ int mmnb_p3m_mesh_size(double a, double grid_spacing)
   if (!(a > 0) || !(grid_spacing > 0))
     return 0;
   return near_2357(floor(a / grid_spacing + 0.5));
+}
+
+// ---- launch tuning ----------------------------------------------------------------
+
+// average time of `iters` replays of a graph of one evaluation at h->d_r
+static int time_evaluation(mmnb_handle *h, int iters, float *ms)
+{
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  h->capturing = true;
+  const long ev = h->evals, ln = h->launches;
+  const int s = mmnb_compute_device(h, h->d_r, h->d_f, h->d_energy);
+  h->capturing = false;
+  const cudaError_t ec = cudaStreamEndCapture(h->stream, &g);
+  h->evals = ev;
+  h->launches = ln;
+  if (s || ec != cudaSuccess) {
+    if (g)
+      cudaGraphDestroy(g);
+    return s ? s : fail(h, MMNB_ERR_CUDA, cudaGetErrorString(ec));
+  }
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+  if (e == cudaSuccess)
+    e = cudaEventCreate(&a);
+  if (e == cudaSuccess)
+    e = cudaEventCreate(&b);
+  for (int k = 0; k < 2 && e == cudaSuccess; k++)
+    e = cudaGraphLaunch(ge, h->stream);
+  if (e == cudaSuccess)
+    e = cudaEventRecord(a, h->stream);
+  for (int k = 0; k < iters && e == cudaSuccess; k++)
+    e = cudaGraphLaunch(ge, h->stream);
+  if (e == cudaSuccess)
+    e = cudaEventRecord(b, h->stream);
+  if (e == cudaSuccess)
+    e = cudaEventSynchronize(b);
+  if (e == cudaSuccess)
+    e = cudaEventElapsedTime(ms, a, b);
+  if (a)
+    cudaEventDestroy(a);
+  if (b)
+    cudaEventDestroy(b);
+  if (ge)
+    cudaGraphExecDestroy(ge);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess)
+    return fail(h, MMNB_ERR_CUDA, std::string("tuning: ") + cudaGetErrorString(e));
+  *ms /= iters;
+  return MMNB_OK;
+}
+
+int mmnb_autotune(mmnb_handle *h, const double *r, int iters)
+{
+  if (!h || !r || iters < 1)
+    return fail(h, MMNB_ERR_ARG, "null handle or positions, or iters < 1");
+  if (!h->params_set)
+    return fail(h, MMNB_ERR_STATE, "mmnb_set_params has not been called");
+  int s;
+  if (h->first && (s = mmnb_compute(h, r, nullptr, nullptr, nullptr, nullptr, nullptr)))
+    return s;
+  const size_t n3 = 3 * (size_t) h->nsite;
+  CK(cudaMemcpyAsync(h->d_r, r, sizeof(double) * n3, cudaMemcpyHostToDevice, h->stream));
+  const bool mixed = h->cfg.precision == MMNB_MIXED;
+  const bool p3m = h->p3m && h->any_q && h->cfg.include_kspace;
+  // one knob at a time, each over its values, keeping the best so far
+  struct Knob {
+    int *v;
+    int vals[2];
+    bool on;
+  } knobs[] = {{&h->tune.water_minb, {4, 5}, mixed && h->water},
+               {&h->tune.spread_planes, {0, 1}, mixed && p3m},
+               {&h->tune.p3m_side, {1, 0}, p3m}};
+  for (Knob &k : knobs) {
+    if (!k.on)
+      continue;
+    int best = *k.v;
+    float best_ms = 0;
+    for (int c = 0; c < 2; c++) {
+      *k.v = k.vals[c];
+      float ms = 0;
+      if ((s = time_evaluation(h, iters, &ms)))
+        return s;
+      if (c == 0 || ms < best_ms) {
+        best_ms = ms;
+        best = k.vals[c];
+      }
+    }
+    *k.v = best;
+  }
+  drop_host_graph(h);
+  CK(cudaStreamSynchronize(h->stream));
+  return MMNB_OK;
+}
+
+int mmnb_get_tuning(mmnb_handle *h, int tuning[3])
+{
+  if (!h || !tuning)
+    return MMNB_ERR_ARG;
+  tuning[0] = h->tune.water_minb;
+  tuning[1] = h->tune.spread_planes;
+  tuning[2] = h->tune.p3m_side;
+  return MMNB_OK;
+}
+
+int mmnb_set_tuning(mmnb_handle *h, const int tuning[3])
+{
+  if (!h || !tuning || (tuning[0] != 4 && tuning[0] != 5) || (tuning[1] != 0 && tuning[1] != 1) ||
+      (tuning[2] != 0 && tuning[2] != 1))
+    return fail(h, MMNB_ERR_ARG, "tuning values: water blocks 4 or 5, spread planes 0 or 1, P3M side 0 or 1");
+  h->tune.water_minb = tuning[0];
+  h->tune.spread_planes = tuning[1];
+  h->tune.p3m_side = tuning[2];
+  drop_host_graph(h);
+  return MMNB_OK;
 }
 
 }  // extern "C"

@@ -44,6 +44,13 @@ constexpr double kFxScale = 4294967296.0;
 constexpr double kFxInv = 1.0 / 4294967296.0;
 constexpr int kAccStride = 8;  // phi, Ex, Ey, Ez, Lx, Ly, Lz, (pad) per site
 
+// Launch choices that do not change any result (mmnb_autotune times them).
+struct Tuning {
+  int water_minb = 4;      // rigid-water pair kernel: 4 or 5 resident blocks per SM
+  int spread_planes = 0;   // mixed P3M spread: 0 one thread per site, 1 P threads per site
+  int p3m_side = 1;        // P3M mesh work on the side stream (1) or in line (0)
+};
+
 // Device buffers of the mixed-precision form.
 struct MixedBufs {
   float4 *site = nullptr;        // sorted, padded slots: offset from the anchor (xyz), charge (w)
@@ -187,6 +194,7 @@ struct mmnb_handle {
   mmnb::MixedBufs mx;
 
   mmnb::Timing timing;
+  mmnb::Tuning tune;
 
   // one captured evaluation (mmnb_graph_capture / mmnb_graph_launch)
   cudaGraph_t graph = nullptr;

@@ -430,6 +430,48 @@ __global__ void k_spread_mixed(MeshArgs m, const double *__restrict__ r, const d
   }
 }
 
+// The same charge assignment with P threads per site, thread a adding the
+// site's plane x = base + a (P^2 adds): P times the parallelism for small
+// systems whose one-thread-per-site grid leaves SMs idle.  Same fixed-point
+// values, so the same mesh.
+template <int P>
+__global__ void k_spread_mixed_planes(MeshArgs m, const double *__restrict__ r, const double *__restrict__ q,
+                                      const int *__restrict__ mask, int nsite, unsigned long long *__restrict__ mesh)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / P, a = t % P;
+  if (i >= nsite || !(mask[i] & MMNB_SITE_HAS_Q))
+    return;
+  const float qi = (float) q[i];
+  const double x = r[3 * i], y = r[3 * i + 1], z = r[3 * i + 2];
+  float W[3][P], ND[3][P];
+  int base[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    double w;
+    base[d] = bspline_base<P>(m.A[d] * x + m.A[3 + d] * y + m.A[6 + d] * z, w);
+    bspline_eval<P, float>((float) w, W[d], ND[d]);
+  }
+  float wa = 0.f;
+#pragma unroll
+  for (int p = 0; p < P; p++)
+    if (p == a)
+      wa = W[0][p];
+  int iz_[P];
+#pragma unroll
+  for (int p = 0; p < P; p++)
+    iz_[p] = wrap_idx(base[2] + p, m.n[2]);
+  const int ix = wrap_idx(base[0] + a, m.n[0]);
+#pragma unroll
+  for (int b = 0; b < P; b++) {
+    const float qw = wa * W[1][b] * qi;
+    unsigned long long *row = mesh + ((size_t) ix * m.n[1] + wrap_idx(base[1] + b, m.n[1])) * m.n[2];
+#pragma unroll
+    for (int c = 0; c < P; c++)
+      atomicAdd(row + iz_[c], (unsigned long long) __float2ll_rn(qw * W[2][c] * 4294967296.0f));
+  }
+}
+
 // fixed-point mesh -> FP32 FFT input; clears the fixed-point mesh for the next step
 __global__ void k_mesh_fx_to_f32(size_t n, unsigned long long *__restrict__ fx, float *__restrict__ out)
 {
@@ -525,8 +567,12 @@ static cudaError_t p3m_mixed_p(mmnb_handle *h, const double *d_r, int stage)
   const size_t nr = (size_t) h->mesh[0] * h->mesh[1] * h->mesh[2];
   const long nk = (long) h->mesh[0] * h->mesh[1] * (h->mesh[2] / 2 + 1);
   if (stage & 1) {
-    k_spread_mixed<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->d_q, h->d_mask, h->nsite,
-                                                                     h->d_mesh_fx);
+    if (h->tune.spread_planes)
+      k_spread_mixed_planes<P><<<div_up(h->nsite * P, 128), 128, 0, h->stream>>>(m, d_r, h->d_q, h->d_mask,
+                                                                                  h->nsite, h->d_mesh_fx);
+    else
+      k_spread_mixed<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->d_q, h->d_mask, h->nsite,
+                                                                       h->d_mesh_fx);
     k_mesh_fx_to_f32<<<div_up((long) nr, 256), 256, 0, h->stream>>>(nr, h->d_mesh_fx, h->d_mesh32);
     timing_mark(h, "p3m_spread");
     if (cufftSetStream(h->plan_r2c32, h->stream) != CUFFT_SUCCESS ||

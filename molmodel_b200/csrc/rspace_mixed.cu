@@ -397,7 +397,10 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-__global__ void __launch_bounds__(kMxWarps * 32, 4) k_pair_water(WaterArgs a)
+// MINB: resident blocks per SM the register budget is cut for (4: 128
+// registers, 5: 96); mmnb_autotune picks per handle
+template <int MINB>
+__global__ void __launch_bounds__(kMxWarps * 32, MINB) k_pair_water(WaterArgs a)
 {
   // per warp: ring of anchor displacement (xyz, r^2), partner O slot (zero
   // offset, charge), H1 and H2 slots (offset, charge); LJ parameters apart
@@ -589,7 +592,10 @@ cudaError_t launch_rspace_water(mmnb_handle *h)
   a.group = h->d_group;
   a.acc = h->mx.acc;
   a.wsum = h->d_wsum;
-  k_pair_water<<<pair_blocks(h), kMxWarps * 32, 0, h->stream>>>(a);
+  if (h->tune.water_minb == 5)
+    k_pair_water<5><<<pair_blocks(h), kMxWarps * 32, 0, h->stream>>>(a);
+  else
+    k_pair_water<4><<<pair_blocks(h), kMxWarps * 32, 0, h->stream>>>(a);
   h->launches += 1;
   return cudaGetLastError();
 }

@@ -137,6 +137,24 @@ class ElecLJ:
         self.energy = dict(elec=e.elec, lj=e.lj, lj_correction=e.lj_correction, total=e.total)
         return uu.value
 
+    def autotune(self, r, iters=10):
+        """Time the launch choices at positions r and keep the fastest;
+        returns them (water-kernel blocks per SM, spread layout, P3M stream)."""
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        check(load().mmnb_autotune(self._h, _d(r), int(iters)), self._h)
+        return self.tuning
+
+    @property
+    def tuning(self):
+        t = np.zeros(3, dtype=np.int32)
+        check(load().mmnb_get_tuning(self._h, _i(t)), self._h)
+        return tuple(int(x) for x in t)
+
+    @tuning.setter
+    def tuning(self, values):
+        t = np.ascontiguousarray(values, dtype=np.int32)
+        check(load().mmnb_set_tuning(self._h, _i(t)), self._h)
+
     def compute_device(self, d_r, d_f, d_energy):
         """Asynchronous evaluation on device pointers (ints), see mmnb_compute_device."""
         check(load().mmnb_compute_device(self._h, ctypes.c_void_p(d_r), ctypes.c_void_p(d_f),

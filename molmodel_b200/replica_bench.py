@@ -75,8 +75,12 @@ def main():
     ap.add_argument("--interval", type=int, default=500)
     ap.add_argument("--precision", default="mixed")
     ap.add_argument("--no-sequential", action="store_true")
+    ap.add_argument("--autotune", action="store_true", help="tune each replica's launch choices first")
     args = ap.parse_args()
     sizes, temps, reps = build(args.replicas, args.precision)
+    tunings = None
+    if args.autotune:
+        tunings = [pot.autotune(wb.positions, iters=5) for wb, pot, _ in reps]
     batch = ReplicaBatch([r[2] for r in reps])
     batch.run(20)  # warm-up (graph capture)
     t0 = time.perf_counter()
@@ -89,6 +93,8 @@ def main():
                replica_steps_per_s=args.replicas * args.steps / t_batch,
                site_steps_per_s=nsite * args.steps / t_batch,
                exchange_acceptance=acc / max(1, att))
+    if tunings is not None:
+        out["tunings"] = {str(t): tunings.count(t) for t in sorted(set(tunings))}
     if not args.no_sequential:
         # the same replicas, each advanced by its own graph in turn (no batching)
         t0 = time.perf_counter()
