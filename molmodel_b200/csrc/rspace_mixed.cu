@@ -379,6 +379,23 @@ __device__ __forceinline__ void water_site(float dx, float dy, float dz, float q
   rinv_out = rinv;
 }
 
+// Minimum-image anchor displacement with contracted FP64 arithmetic (fewer
+// instructions than the reference-rounded form the FP64 kernels use).  The
+// decision it feeds only matters at r = rc, where the switch and its
+// derivative are zero, so the pair set may differ from the FP64 form's only
+// by pairs that contribute nothing.
+__device__ __forceinline__ double anchor_disp_fast(const Box &b, double4 ri, double4 rj, double &x, double &y,
+                                                   double &z)
+{
+  x = ri.x - rj.x;
+  y = ri.y - rj.y;
+  z = ri.z - rj.z;
+  x = fma(-b.L[0], rint(x * b.invL[0]), x);
+  y = fma(-b.L[1], rint(y * b.invL[1]), y);
+  z = fma(-b.L[2], rint(z * b.invL[2]), z);
+  return fma(x, x, fma(y, y, z * z));
+}
+
 __device__ __forceinline__ void cp_async16(void *dst, const void *src)
 {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"((unsigned) __cvta_generic_to_shared(dst)),
@@ -497,8 +514,8 @@ __global__ void __launch_bounds__(kMxWarps * 32, MINB) k_pair_water(WaterArgs a)
       const int e2 = base + 64 + lane;
       const int jnn = e2 < cnt ? row[e2] : p;
       const double4 an = a.anchor[jn];
-      double x, y, z, sx, sy, sz;
-      const double r2a = anchor_disp(a.box, ai, ac, x, y, z, sx, sy, sz);
+      double x, y, z;
+      const double r2a = anchor_disp_fast(a.box, ai, ac, x, y, z);
       const bool take = base + lane < cnt && r2a <= a.rhi2;
       const unsigned bal = __ballot_sync(0xffffffffu, take);
       if (take) {
