@@ -228,6 +228,11 @@ int mmnb_kspace_field_noalloc(int nsite, const double *d_r, const double *d_q, i
                               const double box[3], double eta, double kspace_cutoff,
                               double *d_phi, double *d_evec, void *stream);
 
+/* FP32 FMA throughput of a GPU (TFLOP/s), measured by timing independent FMA
+   chains over the whole device; the denominator of the pair kernels'
+   roofline.  No counterpart in the reference.  device < 0: the current one. */
+int mmnb_measure_fp32_peak(int device, double *tflops);
+
 /* ---- launch tuning ---------------------------------------------------------
    No counterpart in the reference (its path is one CPU thread).  Launch
    choices that change no result: tuning[0] = resident blocks per SM of the

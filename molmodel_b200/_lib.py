@@ -81,6 +81,7 @@ SIGNATURES = [
     ("mmnb_p3m_mesh_size", ctypes.c_int, [ctypes.c_double, ctypes.c_double]),
     ("mmnb_kspace_field_noalloc", ctypes.c_int, [ctypes.c_int, _vp, _vp, ctypes.c_int, _dp, ctypes.c_double,
                                                  ctypes.c_double, _vp, _vp, _vp]),
+    ("mmnb_measure_fp32_peak", ctypes.c_int, [ctypes.c_int, _dp]),
     ("mmnb_autotune", ctypes.c_int, [_vp, _dp, ctypes.c_int]),
     ("mmnb_get_tuning", ctypes.c_int, [_vp, _ip]),
     ("mmnb_set_tuning", ctypes.c_int, [_vp, _ip]),

@@ -26,6 +26,13 @@ def _i(a):
     return a.ctypes.data_as(_ip) if a is not None else None
 
 
+def measure_fp32_peak(device=-1):
+    """FP32 FMA throughput of a GPU in TFLOP/s (mmnb_measure_fp32_peak)."""
+    t = ctypes.c_double(0.0)
+    check(load().mmnb_measure_fp32_peak(int(device), ctypes.byref(t)))
+    return t.value
+
+
 class ElecLJ:
     """Real-space Ewald + LJ with P3M or ordinary-Ewald reciprocal space."""
 
