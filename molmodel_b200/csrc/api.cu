@@ -386,7 +386,8 @@ void free_all(mmnb_handle *h)
                   h->d_phi, h->d_evec, h->d_ljf, h->d_lj_part, h->d_elec_part, h->d_energy, h->d_r, h->d_f,
                   h->d_mesh, h->d_meshk, h->d_green, h->d_kvec, h->d_egrid, h->d_egridk, h->d_mesh32,
                   h->d_meshk32, h->d_green32, h->d_mesh_fx, h->d_kint, h->d_kvecs, h->d_ak, h->d_skc,
-                  h->mx.site, h->mx.par, h->mx.anchor, h->mx.lj, h->mx.acc, h->d_wsum, h->d_bwd};
+                  h->mx.site, h->mx.par, h->mx.anchor, h->mx.lj, h->mx.acc, h->mx.acck, h->d_wsum,
+                  h->d_bwd};
   for (void *p : ptrs)
     if (p)
       cudaFree(p);
@@ -660,7 +661,8 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
   if (c->precision == MMNB_MIXED) {
     if ((s = dalloc(h, &h->mx.site, nslot)) || (s = dalloc(h, &h->mx.par, nslot)) ||
         (s = dalloc(h, &h->mx.anchor, ngroup)) || (s = dalloc(h, &h->mx.lj, ngroup)) ||
-        (s = dalloc(h, &h->mx.acc, (size_t) nsite * kAccStride)))
+        (s = dalloc(h, &h->mx.acc, (size_t) nsite * kAccStride)) ||
+        (s = dalloc(h, &h->mx.acck, (size_t) nsite * 4)))
       return s;
     CK(cudaMemset(h->mx.acc, 0, sizeof(long long) * nsite * kAccStride));
   }
@@ -798,8 +800,9 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
   timing_mark(h, "start");
   // P3M charge assignment and FFTs depend only on the positions: they run on
   // the side stream while the list and pair kernels run here, and are joined
-  // back before interpolation (which adds to what the pair kernels wrote).
-  // With stage timing on, the join follows at once so the marks stay serial.
+  // back before k_finalize (FP64 form: before the interpolation, which adds
+  // to what the pair kernels wrote).  With stage timing on, the join follows
+  // at once so the marks stay serial.
   const bool p3m = h->any_q && h->cfg.include_kspace && h->p3m;
   // the side stream pays off when the pair kernels leave room beside them;
   // mmnb_autotune may put the mesh work in line instead (tune.p3m_side = 0)
@@ -815,8 +818,12 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
       return e;
     return cudaMemsetAsync(h->d_ljf, 0, sizeof(double) * 3 * h->nsite, h->stream);
   };
+  // the mixed form's interpolation writes words of its own (k_gather_mixed),
+  // so it joins the mesh work; the FP64 interpolation adds into the site
+  // arrays the pair kernels write and waits for them
+  const int mesh_stages = mixed ? 3 : 1;
   if (p3m && !side)
-    CK(mixed ? launch_p3m_mixed(h, d_r, 1) : launch_p3m_fp64(h, d_r, 1));
+    CK(mixed ? launch_p3m_mixed(h, d_r, mesh_stages) : launch_p3m_fp64(h, d_r, mesh_stages));
   if (side) {
     cudaStream_t main = h->stream;
     CK(cudaEventRecord(h->ev_fork, main));
@@ -830,7 +837,7 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
       timing_mark(h, "rspace_excl");
     }
     if (e == cudaSuccess)
-      e = mixed ? launch_p3m_mixed(h, d_r, 1) : launch_p3m_fp64(h, d_r, 1);
+      e = mixed ? launch_p3m_mixed(h, d_r, mesh_stages) : launch_p3m_fp64(h, d_r, mesh_stages);
     h->stream = main;
     CK(e);
     CK(cudaEventRecord(h->ev_join, h->side));
@@ -871,7 +878,8 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
   if (p3m) {
     if (side && !h->timing.on)
       CK(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
-    CK(mixed ? launch_p3m_mixed(h, d_r, 2) : launch_p3m_fp64(h, d_r, 2));
+    if (!mixed)
+      CK(launch_p3m_fp64(h, d_r, 2));
     timing_mark(h, "kspace");
   } else if (h->any_q && h->cfg.include_kspace && h->kspace) {
     CK(launch_kspace(h, d_r));

@@ -18,6 +18,7 @@ struct FinArgs {
   double self_a, neutral_b;
   const double *q;
   const long long *acc;  // mixed form: fixed-point potential, field and LJ force per site
+  const long long *acck; // mixed P3M: fixed-point interpolated potential and field per site
   double *phi, *evec, *ljf, *f, *elec_part;
   // energy reduction
   const double *lj_part;              // per-block LJ partials [lj_lo, lj_hi)
@@ -54,9 +55,17 @@ __global__ void __launch_bounds__(kFinThreads) k_finalize(FinArgs a)
     if (a.acc) {
       // fold the fixed-point sums into the FP64 site arrays
       const long long *o = a.acc + (size_t) i * kAccStride;
-      p += (double) o[0] * kFxInv;
+      long long k[4] = {0, 0, 0, 0};
+      if (a.acck) {
+        const longlong4 v = reinterpret_cast<const longlong4 *>(a.acck)[i];
+        k[0] = v.x;
+        k[1] = v.y;
+        k[2] = v.z;
+        k[3] = v.w;
+      }
+      p += (double) (o[0] + k[0]) * kFxInv;
       for (int d = 0; d < 3; d++) {
-        a.evec[3 * i + d] += (double) o[1 + d] * kFxInv;
+        a.evec[3 * i + d] += (double) (o[1 + d] + k[1 + d]) * kFxInv;
         a.ljf[3 * i + d] += (double) o[4 + d] * kFxInv;
       }
     }
@@ -115,6 +124,7 @@ cudaError_t launch_finalize(mmnb_handle *h, double *d_f, double *d_energy)
   a.neutral_b = h->neutral_b;
   a.q = h->d_q;
   a.acc = h->cfg.precision == MMNB_MIXED ? h->mx.acc : nullptr;
+  a.acck = (a.acc && h->any_q && h->cfg.include_kspace && h->p3m) ? h->mx.acck : nullptr;
   a.phi = h->d_phi;
   a.evec = h->d_evec;
   a.ljf = h->d_ljf;

@@ -58,6 +58,7 @@ struct MixedBufs {
   double4 *anchor = nullptr;     // sorted groups: anchor position (FP64)
   float2 *lj = nullptr;          // sorted groups: anchor sigma, sqrt(epsilon)
   long long *acc = nullptr;      // per site (original order), kAccStride fixed-point values
+  long long *acck = nullptr;     // per site (original order): P3M interpolation phi, Ex, Ey, Ez
 };
 
 // Stage timing with CUDA events recorded on the handle's stream.  Each

@@ -501,9 +501,12 @@ __global__ void k_green_to_f32(long nk, const double *__restrict__ green, float 
     out[g] = (float) green[g];
 }
 
+// Interpolation writes its own fixed-point words (phi, Ex, Ey, Ez per site),
+// which k_finalize adds to the pair kernels' sums: it touches nothing the
+// pair kernels write, so it runs on the side stream beside them.
 template <int P>
 __global__ void k_gather_mixed(MeshArgs m, const double *__restrict__ r, int nsite, const float *__restrict__ mesh,
-                               long long *__restrict__ acc)
+                               long long *__restrict__ acck)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nsite)
@@ -546,11 +549,12 @@ __global__ void k_gather_mixed(MeshArgs m, const double *__restrict__ r, int nsi
     }
   }
   const float A0 = (float) m.A[0], A4 = (float) m.A[4], A8 = (float) m.A[8];
-  long long *o = acc + (size_t) i * kAccStride;
-  o[0] += __float2ll_rn(ph * 4294967296.0f);
-  o[1] += __float2ll_rn(gx * A0 * 4294967296.0f);
-  o[2] += __float2ll_rn(gy * A4 * 4294967296.0f);
-  o[3] += __float2ll_rn(gz * A8 * 4294967296.0f);
+  longlong4 o;
+  o.x = __float2ll_rn(ph * 4294967296.0f);
+  o.y = __float2ll_rn(gx * A0 * 4294967296.0f);
+  o.z = __float2ll_rn(gy * A4 * 4294967296.0f);
+  o.w = __float2ll_rn(gz * A8 * 4294967296.0f);
+  reinterpret_cast<longlong4 *>(acck)[i] = o;
 }
 
 cudaError_t launch_green32(mmnb_handle *h)
@@ -586,7 +590,7 @@ static cudaError_t p3m_mixed_p(mmnb_handle *h, const double *d_r, int stage)
     h->launches += 3;
   }
   if (stage & 2) {
-    k_gather_mixed<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->nsite, h->d_mesh32, h->mx.acc);
+    k_gather_mixed<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->nsite, h->d_mesh32, h->mx.acck);
     timing_mark(h, "p3m_gather");
     h->launches += 1;
   }
