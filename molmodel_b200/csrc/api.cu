@@ -381,7 +381,7 @@ void free_all(mmnb_handle *h)
   void *ptrs[] = {h->d_group, h->d_excl_ptr, h->d_excl_idx, h->d_p14_ptr, h->d_p14_idx, h->d_gexcl_ptr,
                   h->d_gexcl_idx, h->d_mask, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_cheb,
                   h->d_stencil, h->d_cell_rank, h->d_cell_of_rank, h->d_cell_of_group, h->d_cell_count,
-                  h->d_cell_start, h->d_slot, h->d_sorted, h->d_rank, h->d_anchor, h->d_last, h->d_anchor_sorted,
+                  h->d_cell_start, h->d_slot, h->d_sorted, h->d_rank, h->d_anchor, h->d_last, h->d_anchor_sorted, h->d_anchor32, h->d_block_sum,
                   h->d_top2, h->d_nbr, h->d_nbr_count, h->d_flags, h->d_sr, h->d_sp, h->d_site_of_slot,
                   h->d_phi, h->d_evec, h->d_ljf, h->d_lj_part, h->d_elec_part, h->d_energy, h->d_r, h->d_f,
                   h->d_mesh, h->d_meshk, h->d_green, h->d_kvec, h->d_egrid, h->d_egridk, h->d_mesh32,
@@ -633,9 +633,18 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
   if ((s = dalloc(h, &h->d_cell_of_group, ngroup)) || (s = dalloc(h, &h->d_slot, ngroup)) ||
       (s = dalloc(h, &h->d_sorted, ngroup)) || (s = dalloc(h, &h->d_rank, ngroup)) ||
       (s = dalloc(h, &h->d_anchor, 3 * (size_t) ngroup)) || (s = dalloc(h, &h->d_last, 3 * (size_t) ngroup)) ||
-      (s = dalloc(h, &h->d_anchor_sorted, 3 * (size_t) ngroup)) || (s = dalloc(h, &h->d_nbr_count, ngroup)) ||
-      (s = dalloc(h, &h->d_flags, kFlagCount)))
+      (s = dalloc(h, &h->d_anchor_sorted, 3 * (size_t) ngroup)) || (s = dalloc(h, &h->d_anchor32, ngroup)) ||
+      (s = dalloc(h, &h->d_nbr_count, ngroup)) || (s = dalloc(h, &h->d_flags, kFlagCount)))
     return s;
+  {
+    // one word per block of the cooperative rebuild (at most 2048 threads of
+    // 256-thread blocks resident per SM)
+    int nsm = 0;
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->dev));
+    h->block_sum_cap = 8 * nsm;
+    if ((s = dalloc(h, &h->d_block_sum, (size_t) h->block_sum_cap)))
+      return s;
+  }
   CK(cudaMemset(h->d_last, 0, sizeof(double) * 3 * ngroup));
   CK(cudaMemset(h->d_flags, 0, sizeof(int) * kFlagCount));
   CK(cudaMallocHost((void **) &h->h_flags, sizeof(int) * kFlagCount));

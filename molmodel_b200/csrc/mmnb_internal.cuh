@@ -130,9 +130,12 @@ struct mmnb_handle {
   double *d_anchor = nullptr;        // 3*ngroup current anchors (original order)
   double *d_last = nullptr;          // 3*ngroup anchors at the last rebuild
   double *d_anchor_sorted = nullptr; // 3*ngroup anchors at the last rebuild, sorted order
+  float4 *d_anchor32 = nullptr;      // the same, wrapped into the box, FP32 (list pre-test)
   double *d_top2 = nullptr;          // per-block top-2 displacements
   int top2_blocks = 0;
   int rebuild_grid = 0;              // blocks of the cooperative rebuild launch (0: not sized yet)
+  int *d_block_sum = nullptr;        // per rebuild block: its segment's cell count
+  int block_sum_cap = 0;
   int rowcap = 0;
   int *d_nbr = nullptr;              // ngroup * rowcap, sorted positions
   int *d_nbr_count = nullptr;        // ngroup

@@ -15,13 +15,19 @@
 // The arithmetic that decides membership (cell index, squared distance,
 // displacement test) uses explicitly rounded FP64 operations so it cannot be
 // contracted into FMAs: it is the same IEEE sequence the reference executes,
-// and the pair set is identical, not merely close.
+// and the pair set is identical, not merely close.  The list build first
+// tests each candidate in FP32 against a band around (cutoff + width)^2 wide
+// enough to hold every FP32 rounding error; only candidates inside the band
+// take the FP64 test, so the decision is the FP64 one.
 //
 // The list is stored FULL (each unordered pair in both rows) so the pair
 // kernels accumulate on their own rows only, without atomics.  Rows are
 // indexed by sorted position (groups ordered by the Morton rank of their cell).
 
 #include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cmath>
 
 #include "mmnb_internal.cuh"
 
@@ -145,6 +151,15 @@ struct RebuildArgs {
   int *cell_of_group, *cell_count, *slot, *start, *sorted, *rank;
   double *last, *anchor_sorted;
   int *nbr, *nbr_count;
+  // FP32 pre-test of the list build: sorted anchors wrapped into the box, and
+  // squared distances that are certainly inside (< c2lo) or outside (> c2hi)
+  // of (cutoff + width)^2 whatever the FP32 rounding; only the rest take the
+  // exact FP64 test, so the pair set is the same
+  float4 *anchor32;
+  float Lf[3], invLf[3];
+  float c2lo, c2hi;
+  int *block_sum;            // per block of the launch: its segment's cell count
+  int *scatter;              // groups by cell before the in-cell ordering (ngroup)
 };
 
 constexpr int kRebuildThreads = 256;
@@ -168,105 +183,199 @@ __device__ __forceinline__ void cell_assign(const RebuildArgs &a, int g)
   a.slot[g] = atomicAdd(&a.cell_count[a.cell_rank[c]], 1);
 }
 
-// exclusive scan of the per-rank counts by one block
-__device__ void scan_cells(const RebuildArgs &a, int *part)
+// Exclusive scan of the 256 values of a block (one per thread); returns the
+// thread's exclusive prefix and the block total in *total.
+__device__ __forceinline__ int block_exclusive_scan(int v, int *warp_tot, int *total)
 {
-  const int nt = blockDim.x;
-  const int per = (a.ncell3 + nt - 1) / nt;
-  const int beg = threadIdx.x * per;
-  const int end = min(beg + per, a.ncell3);
-  int s = 0;
-  for (int i = beg; i < end; i++)
-    s += a.cell_count[i];
-  part[threadIdx.x] = s;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o)
+      incl += u;
+  }
+  if (lane == 31)
+    warp_tot[w] = incl;
   __syncthreads();
-  // Hillis-Steele inclusive scan of the partial sums
-  for (int off = 1; off < nt; off <<= 1) {
-    const int v = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
-    __syncthreads();
-    part[threadIdx.x] += v;
-    __syncthreads();
+  int before = 0, all = 0;
+  for (int k = 0; k < kRebuildThreads / 32; k++) {
+    const int t = warp_tot[k];
+    before += k < w ? t : 0;
+    all += t;
   }
-  int run = threadIdx.x > 0 ? part[threadIdx.x - 1] : 0;
-  for (int i = beg; i < end; i++) {
-    a.start[i] = run;
-    run += a.cell_count[i];
-  }
-  if (threadIdx.x == nt - 1)
-    a.start[a.ncell3] = part[nt - 1];
+  __syncthreads();
+  *total = all;
+  return before + incl - v;
 }
 
-// order a cell's members by group index (deterministic lists), then record
-// sorted positions and the anchors the list is built from
-__device__ __forceinline__ void cell_finish(const RebuildArgs &a, int c)
+// Counting-sort offsets over the whole grid: each block sums a contiguous
+// segment of the per-rank cell counts (phase 1); after a grid barrier each
+// block adds the sums of the blocks before it and scans its segment (phase 2).
+__device__ __forceinline__ void scan_segment(const RebuildArgs &a, int &lo, int &hi)
 {
-  const int b = a.start[c], e = a.start[c + 1];
-  for (int i = b + 1; i < e; i++) {
-    const int v = a.sorted[i];
-    int j = i - 1;
-    while (j >= b && a.sorted[j] > v) {
-      a.sorted[j + 1] = a.sorted[j];
-      j--;
-    }
-    a.sorted[j + 1] = v;
-  }
-  for (int i = b; i < e; i++) {
-    const int g = a.sorted[i];
-    a.rank[g] = i;
-    a.anchor_sorted[3 * i] = a.last[3 * g];
-    a.anchor_sorted[3 * i + 1] = a.last[3 * g + 1];
-    a.anchor_sorted[3 * i + 2] = a.last[3 * g + 2];
-  }
+  const int seg = (a.ncell3 + gridDim.x - 1) / gridDim.x;
+  lo = min(a.ncell3, (int) blockIdx.x * seg);
+  hi = min(a.ncell3, lo + seg);
 }
 
-// one warp per sorted group; lanes walk stencil cells, members are compacted
-// into the row with a ballot
-__device__ __forceinline__ void build_row(const RebuildArgs &a, int p, int lane)
+__device__ void scan_cells_sum(const RebuildArgs &a, int *warp_tot)
+{
+  int lo, hi;
+  scan_segment(a, lo, hi);
+  int v = 0;
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x)
+    v += a.cell_count[i];
+  int total;
+  block_exclusive_scan(v, warp_tot, &total);
+  if (threadIdx.x == 0)
+    a.block_sum[blockIdx.x] = total;
+}
+
+__device__ void scan_cells_write(const RebuildArgs &a, int *warp_tot)
+{
+  int lo, hi;
+  scan_segment(a, lo, hi);
+  int v = 0;
+  for (int k = threadIdx.x; k < (int) blockIdx.x; k += blockDim.x)
+    v += a.block_sum[k];
+  int run;
+  block_exclusive_scan(v, warp_tot, &run);
+  for (int i0 = lo; i0 < hi; i0 += blockDim.x) {
+    const int i = i0 + threadIdx.x;
+    const int c = i < hi ? a.cell_count[i] : 0;
+    int tile;
+    const int ex = block_exclusive_scan(c, warp_tot, &tile);
+    if (i < hi)
+      a.start[i] = run + ex;
+    run += tile;
+  }
+  // the last block's running offset ends at the total
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0)
+    a.start[a.ncell3] = run;
+}
+
+// Final sorted position of the group scattered to position i (members of a
+// cell ordered by group index: deterministic lists), its rank, and the
+// anchors the list is built from.
+__device__ __forceinline__ void place_group(const RebuildArgs &a, int i)
+{
+  const int g = a.scatter[i];
+  const int rj = a.cell_rank[a.cell_of_group[g]];
+  const int b = a.start[rj], e = a.start[rj + 1];
+  int r = 0;
+  for (int j = b; j < e; j++)
+    r += a.scatter[j] < g;
+  const int pos = b + r;
+  a.sorted[pos] = g;
+  a.rank[g] = pos;
+  float w[3];
+  for (int d = 0; d < 3; d++) {
+    const double x = a.last[3 * g + d];
+    a.anchor_sorted[3 * pos + d] = x;
+    w[d] = (float) (x - a.box.L[d] * floor(x * a.box.invL[d]));
+  }
+  a.anchor32[pos] = make_float4(w[0], w[1], w[2], 0.f);
+}
+
+// one warp per sorted group.  Per batch of 32 stencil cells the members are
+// laid out in one candidate sequence (cell order, then member order; a warp
+// scan of the cells' counts gives each cell's offset), the lanes test
+// consecutive candidates, and the accepted ones are compacted into the row
+// with a ballot.  Rows are in a fixed order (deterministic lists).
+constexpr int kCand = 128;  // candidates staged per warp at a time
+constexpr int kSeg = 256;   // stencil cells whose member ranges a warp fetches at a time
+
+__device__ __forceinline__ void build_row(const RebuildArgs &a, int p, int lane, int *cand, int2 *ranges)
 {
   const int n = a.cg.n;
   const int gi = a.sorted[p];
   const int ci = a.cell_of_group[gi];
   const int ix = ci / (n * n), iy = (ci / n) % n, iz = ci % n;
   const double xi = a.anchor_sorted[3 * p], yi = a.anchor_sorted[3 * p + 1], zi = a.anchor_sorted[3 * p + 2];
+  const float4 wi = a.anchor32[p];
   int *row = a.nbr + (size_t) p * a.rowcap;
   const unsigned below = (1u << lane) - 1;
   int count = 0;
-  for (int s0 = 0; s0 < a.nstencil; s0 += 32) {
-    const int s = s0 + lane;
-    int beg = 0, end = 0;
-    if (s < a.nstencil) {
+  for (int g0 = 0; g0 < a.nstencil; g0 += kSeg) {
+    // the member ranges of a segment of stencil cells, fetched with independent
+    // loads (one dependent chain per cell instead of one per batch of 32)
+    const int segn = min(kSeg, a.nstencil - g0);
+#pragma unroll 4
+    for (int t = lane; t < segn; t += 32) {
+      const int s = g0 + t;
       const int jx = (ix + a.stencil[3 * s]) % n;
       const int jy = (iy + a.stencil[3 * s + 1]) % n;
       const int jz = (iz + a.stencil[3 * s + 2]) % n;
       const int rj = a.cell_rank[(jx * n + jy) * n + jz];
-      beg = a.start[rj];
-      end = a.start[rj + 1];
+      ranges[t] = make_int2(a.start[rj], a.start[rj + 1]);
     }
-    const bool same = (s == 0);
-    for (int m = 0;; m++) {
-      const int q = beg + m;
-      const bool has = q < end;
-      if (!__any_sync(0xffffffffu, has))
-        break;
-      bool take = false;
-      if (has && q != p) {
-        if (same) {
-          take = true;
-        } else {
-          const double dx = exact_wrap(__dsub_rn(xi, a.anchor_sorted[3 * q]), a.box.L[0], a.box.invL[0]);
-          const double dy = exact_wrap(__dsub_rn(yi, a.anchor_sorted[3 * q + 1]), a.box.L[1], a.box.invL[1]);
-          const double dz = exact_wrap(__dsub_rn(zi, a.anchor_sorted[3 * q + 2]), a.box.L[2], a.box.invL[2]);
-          take = exact_sq3(dx, dy, dz) < a.cg.c2;
+    __syncwarp();
+    for (int b0 = 0; b0 < segn; b0 += 32) {
+      const int s0 = g0 + b0;
+      int beg = 0, end = 0;
+      if (b0 + lane < segn) {
+        const int2 rg = ranges[b0 + lane];
+        beg = rg.x;
+        end = rg.y;
+      }
+      const int c = end - beg;
+      int incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o)
+          incl += v;
+      }
+      const int excl = incl - c;
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      // stencil entry 0 is the group's own cell: its members pair unconditionally
+      const int own = s0 == 0 ? __shfl_sync(0xffffffffu, incl, 0) : 0;
+      for (int base = 0; base < total; base += kCand) {
+        const int lo = max(excl, base), hi = min(incl, base + kCand);
+        for (int k = lo; k < hi; k++)
+          cand[k - base] = beg + (k - excl);
+        __syncwarp();
+        const int nb = min(kCand, total - base);
+        for (int k0 = 0; k0 < nb; k0 += 32) {
+          const int k = k0 + lane;
+          bool take = false;
+          int q = 0;
+          if (k < nb) {
+            q = cand[k];
+            if (q != p) {
+              if (base + k < own) {
+                take = true;
+              } else {
+                const float4 wj = a.anchor32[q];
+                float fx = wi.x - wj.x, fy = wi.y - wj.y, fz = wi.z - wj.z;
+                fx -= a.Lf[0] * rintf(fx * a.invLf[0]);
+                fy -= a.Lf[1] * rintf(fy * a.invLf[1]);
+                fz -= a.Lf[2] * rintf(fz * a.invLf[2]);
+                const float f2 = fx * fx + fy * fy + fz * fz;
+                if (f2 < a.c2lo) {
+                  take = true;
+                } else if (f2 <= a.c2hi) {
+                  const double dx = exact_wrap(__dsub_rn(xi, a.anchor_sorted[3 * q]), a.box.L[0], a.box.invL[0]);
+                  const double dy = exact_wrap(__dsub_rn(yi, a.anchor_sorted[3 * q + 1]), a.box.L[1], a.box.invL[1]);
+                  const double dz = exact_wrap(__dsub_rn(zi, a.anchor_sorted[3 * q + 2]), a.box.L[2], a.box.invL[2]);
+                  take = exact_sq3(dx, dy, dz) < a.cg.c2;
+                }
+              }
+            }
+          }
+          const unsigned bal = __ballot_sync(0xffffffffu, take);
+          if (take) {
+            const int idx = count + __popc(bal & below);
+            if (idx < a.rowcap)
+              row[idx] = q;
+          }
+          count += __popc(bal);
         }
+        __syncwarp();
       }
-      const unsigned bal = __ballot_sync(0xffffffffu, take);
-      if (take) {
-        const int idx = count + __popc(bal & below);
-        if (idx < a.rowcap)
-          row[idx] = q;
-      }
-      count += __popc(bal);
     }
+    __syncwarp();
   }
   if (lane == 0) {
     a.nbr_count[p] = min(count, a.rowcap);
@@ -277,8 +386,8 @@ __device__ __forceinline__ void build_row(const RebuildArgs &a, int p, int lane)
 }
 
 // The whole rebuild in one cooperative launch: cell assignment, counting-sort
-// scan, scatter, per-cell ordering, list rows, separated by grid-wide
-// barriers.  Without a rebuild due every block returns at once (the decision
+// scan (block sums, then offsets), scatter, placement in group order within
+// each cell, list rows, separated by grid-wide barriers.  Without a rebuild due every block returns at once (the decision
 // is read from device memory, so the launch sits in a CUDA graph unchanged).
 __global__ void __launch_bounds__(kRebuildThreads) k_list_rebuild(RebuildArgs a)
 {
@@ -286,23 +395,26 @@ __global__ void __launch_bounds__(kRebuildThreads) k_list_rebuild(RebuildArgs a)
     return;
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
-  __shared__ int part[kRebuildThreads];
+  __shared__ int warp_tot[kBuildWarps];
+  __shared__ int cand[kBuildWarps * kCand];
+  __shared__ int2 ranges[kBuildWarps * kSeg];
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   for (int g = tid; g < a.ngroup; g += nth)
     cell_assign(a, g);
   grid.sync();
-  if (blockIdx.x == 0)
-    scan_cells(a, part);
+  scan_cells_sum(a, warp_tot);
+  grid.sync();
+  scan_cells_write(a, warp_tot);
   grid.sync();
   for (int g = tid; g < a.ngroup; g += nth)
-    a.sorted[a.start[a.cell_rank[a.cell_of_group[g]]] + a.slot[g]] = g;
+    a.scatter[a.start[a.cell_rank[a.cell_of_group[g]]] + a.slot[g]] = g;
   grid.sync();
-  for (int c = tid; c < a.ncell3; c += nth)
-    cell_finish(a, c);
+  for (int i = tid; i < a.ngroup; i += nth)
+    place_group(a, i);
   grid.sync();
   const int lane = threadIdx.x & 31;
   for (int p = tid >> 5; p < a.ngroup; p += nth >> 5)
-    build_row(a, p, lane);
+    build_row(a, p, lane, cand + (threadIdx.x >> 5) * kCand, ranges + (threadIdx.x >> 5) * kSeg);
 }
 
 cudaError_t launch_list_check(mmnb_handle *h, const double *d_r, int force)
@@ -325,7 +437,7 @@ cudaError_t launch_list_rebuild(mmnb_handle *h)
       return e;
     if (per_sm < 1)
       return cudaErrorLaunchOutOfResources;
-    h->rebuild_grid = std::min(per_sm * nsm, div_up(h->ngroup, kBuildWarps));
+    h->rebuild_grid = std::min(std::min(per_sm * nsm, div_up(h->ngroup, kBuildWarps)), h->block_sum_cap);
   }
   RebuildArgs a;
   a.ngroup = h->ngroup;
@@ -348,6 +460,27 @@ cudaError_t launch_list_rebuild(mmnb_handle *h)
   a.anchor_sorted = h->d_anchor_sorted;
   a.nbr = h->d_nbr;
   a.nbr_count = h->d_nbr_count;
+  a.anchor32 = h->d_anchor32;
+  a.block_sum = h->d_block_sum;
+  // the rows' counts are written last, by the list build: until then they
+  // hold the groups in cell order
+  a.scatter = h->d_nbr_count;
+  // bound of the FP32 squared-distance error: anchors wrapped into [0, L] and
+  // rounded (<= 4 ulp(L) per component after the difference and the image
+  // shift), propagated through |d|^2, plus the rounding of the sum; 8x margin
+  double lmax = 0, lmin = 1e300;
+  for (int d = 0; d < 3; d++) {
+    a.Lf[d] = (float) h->box.L[d];
+    a.invLf[d] = (float) h->box.invL[d];
+    lmax = std::max(lmax, h->box.L[d]);
+    lmin = std::min(lmin, h->box.L[d]);
+  }
+  const double c2 = h->cg.c2, ulp = std::ldexp(1.0, -23);
+  const double tol = 8 * (2 * std::sqrt(3.0) * std::sqrt(c2) * 4 * ulp * lmax + 4 * ulp * c2);
+  // the FP32 minimum image may pick another image only at |d| ~ L/2
+  const bool safe = std::sqrt(c2) + 1.0 < 0.45 * lmin;
+  a.c2lo = safe ? (float) (c2 - tol) : -1.0f;
+  a.c2hi = safe ? (float) (c2 + tol) : 3.0e38f;
   void *args[] = {&a};
   h->launches += 1;
   return cudaLaunchCooperativeKernel((const void *) k_list_rebuild, dim3(h->rebuild_grid), dim3(kRebuildThreads),
