@@ -278,8 +278,9 @@ def run_ours(args):
            "config": {"workload": WORKLOAD, "precision": args.precision, "l2": "flushed (256 MB write) before every "
                       "timed step", "parallelism": f"replicas x{world}", "dt_fs_for_ns_per_day": DT_FS,
                       "launch": "CUDA graph of one evaluation, replayed per step",
-                      "tuning": {"water_kernel_blocks_per_sm": tuning[0], "spread_threads_per_site":
-                                 "P" if tuning[1] else "1", "p3m_side_stream": bool(tuning[2])}},
+                      "tuning": {"water_kernel_blocks_per_sm": tuning[0], "spread_layout":
+                                 ("thread per site", "thread per site and x-plane",
+                                  "lane per site and z-offset")[tuning[1]], "p3m_side_stream": bool(tuning[2])}},
            "ms_per_step_without_graph": nograph_ms / args.steps,
            "pair_evals_per_s": work["coulomb_site_pairs"] * steps_per_s,
            "ns_per_day": steps_per_s / world * DT_FS * 86400 / 1e6,

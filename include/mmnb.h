@@ -236,8 +236,10 @@ int mmnb_measure_fp32_peak(int device, double *tflops);
 /* ---- launch tuning ---------------------------------------------------------
    No counterpart in the reference (its path is one CPU thread).  Launch
    choices that change no result: tuning[0] = resident blocks per SM of the
-   rigid-water pair kernel (4 or 5: its register budget), tuning[1] = threads
-   per site of the mixed P3M charge assignment (0: one, 1: one per mesh plane),
+   rigid-water pair kernel (4 or 5: its register budget), tuning[1] = layout
+   of the mixed P3M charge assignment (0: a thread per site, 1: a thread per
+   site and mesh x-plane, 2 (default): a lane per site and mesh z-offset, so
+   the lanes of a site reduce into consecutive mesh words),
    tuning[2] = P3M mesh work on a second stream beside the pair kernels (1) or
    in line (0).  mmnb_autotune times each choice over `iters` graph replays of
    an evaluation at r (host array) and keeps the fastest; small systems gain

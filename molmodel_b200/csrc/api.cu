@@ -1375,17 +1375,18 @@ int mmnb_autotune(mmnb_handle *h, const double *r, int iters)
   // one knob at a time, each over its values, keeping the best so far
   struct Knob {
     int *v;
-    int vals[2];
+    int nval;
+    int vals[3];
     bool on;
-  } knobs[] = {{&h->tune.water_minb, {4, 5}, mixed && h->water},
-               {&h->tune.spread_planes, {0, 1}, mixed && p3m},
-               {&h->tune.p3m_side, {1, 0}, p3m}};
+  } knobs[] = {{&h->tune.water_minb, 2, {4, 5}, mixed && h->water},
+               {&h->tune.spread_planes, 3, {2, 0, 1}, mixed && p3m},
+               {&h->tune.p3m_side, 2, {1, 0}, p3m}};
   for (Knob &k : knobs) {
     if (!k.on)
       continue;
     int best = *k.v;
     float best_ms = 0;
-    for (int c = 0; c < 2; c++) {
+    for (int c = 0; c < k.nval; c++) {
       *k.v = k.vals[c];
       float ms = 0;
       if ((s = time_evaluation(h, iters, &ms)))
@@ -1414,9 +1415,9 @@ int mmnb_get_tuning(mmnb_handle *h, int tuning[3])
 
 int mmnb_set_tuning(mmnb_handle *h, const int tuning[3])
 {
-  if (!h || !tuning || (tuning[0] != 4 && tuning[0] != 5) || (tuning[1] != 0 && tuning[1] != 1) ||
+  if (!h || !tuning || (tuning[0] != 4 && tuning[0] != 5) || tuning[1] < 0 || tuning[1] > 2 ||
       (tuning[2] != 0 && tuning[2] != 1))
-    return fail(h, MMNB_ERR_ARG, "tuning values: water blocks 4 or 5, spread planes 0 or 1, P3M side 0 or 1");
+    return fail(h, MMNB_ERR_ARG, "tuning values: water blocks 4 or 5, spread layout 0, 1 or 2, P3M side 0 or 1");
   h->tune.water_minb = tuning[0];
   h->tune.spread_planes = tuning[1];
   h->tune.p3m_side = tuning[2];

@@ -20,7 +20,7 @@ def test_every_tuning_gives_the_same_result():
     wb = water_box(10, seed=6)
     p = _pot(wb)
     ref = p.compute(wb.positions)
-    for combo in itertools.product((4, 5), (0, 1), (1, 0)):
+    for combo in itertools.product((4, 5), (0, 1, 2), (1, 0)):
         p.tuning = combo
         assert p.tuning == combo
         g = p.compute(wb.positions)   # host call: graph replay with these choices
@@ -35,7 +35,7 @@ def test_autotune_keeps_valid_choices():
     p = _pot(wb)
     before = p.compute(wb.positions)
     t = p.autotune(wb.positions, iters=5)
-    assert t[0] in (4, 5) and t[1] in (0, 1) and t[2] in (0, 1)
+    assert t[0] in (4, 5) and t[1] in (0, 1, 2) and t[2] in (0, 1)
     after = p.compute(wb.positions)
     assert np.array_equal(before["f"], after["f"])
     p.close()
