@@ -617,7 +617,14 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
   CK(cudaGetDevice(&h->dev));
   CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
   h->stream = h->own_stream;
-  CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+  {
+    // the mesh work on the side stream at the highest priority: its blocks
+    // go first whenever the pair kernels' blocks leave an SM slot (graphs are
+    // instantiated with node priorities so captured launches keep it)
+    int least = 0, greatest = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    CK(cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, greatest));
+  }
   CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
   int s;
@@ -816,9 +823,8 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
   // the side stream pays off when the pair kernels leave room beside them;
   // mmnb_autotune may put the mesh work in line instead (tune.p3m_side = 0)
   const bool side = p3m && h->tune.p3m_side;
-  // the mixed form's FP64 site arrays (zeroed here, then the exclusion
-  // corrections) do not meet the pair kernels either: they go to the side
-  // stream too
+  // the mixed form's FP64 site arrays (written by the exclusion corrections)
+  // do not meet the pair kernels either: they go to the side stream too
   const bool excl_side = side && mixed && h->cfg.include_rspace;
   auto zero_site_arrays = [&]() -> cudaError_t {
     cudaError_t e;
@@ -840,9 +846,7 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
     h->stream = h->side;
     cudaError_t e = cudaSuccess;
     if (excl_side) {
-      e = zero_site_arrays();
-      if (e == cudaSuccess)
-        e = launch_exclusions(h, d_r);
+      e = launch_exclusions(h, d_r);
       timing_mark(h, "rspace_excl");
     }
     if (e == cudaSuccess)
@@ -856,8 +860,10 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
   CK(launch_list_check(h, d_r, h->force_rebuild_next));
   CK(launch_list_rebuild(h));
   timing_mark(h, "nbrlist");
-  // FP64 site arrays collect the terms the fixed-point sums do not hold
-  if ((mixed || !h->cfg.include_rspace) && !excl_side)
+  // FP64 site arrays collect the terms the fixed-point sums do not hold; their
+  // first writer (FP64 pair kernels, or the mixed form's exclusion
+  // corrections) assigns them, so they need clearing only without real space
+  if (!h->cfg.include_rspace)
     CK(zero_site_arrays());
   if (mixed)
     CK(launch_prep_mixed(h, d_r));
@@ -934,7 +940,7 @@ int mmnb_graph_capture(mmnb_handle *h, const double *d_r, double *d_f, double *d
   if (e != cudaSuccess)
     return fail(h, MMNB_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
   h->graph = g;
-  CK(cudaGraphInstantiate(&h->graph_exec, h->graph, 0));
+  CK(cudaGraphInstantiate(&h->graph_exec, h->graph, cudaGraphInstantiateFlagUseNodePriority));
   return MMNB_OK;
 }
 
@@ -994,7 +1000,7 @@ int mmnb_compute(mmnb_handle *h, const double *r, double *f, double *u, mmnb_ene
         return fail(h, MMNB_ERR_CUDA, std::string("capture of the host call: ") + cudaGetErrorString(ec));
       }
       h->hgraph = g;
-      CK(cudaGraphInstantiate(&h->hgraph_exec, g, 0));
+      CK(cudaGraphInstantiate(&h->hgraph_exec, g, cudaGraphInstantiateFlagUseNodePriority));
     }
     if (graph) {
       CK(cudaGraphLaunch(h->hgraph_exec, h->stream));
@@ -1329,7 +1335,7 @@ static int time_evaluation(mmnb_handle *h, int iters, float *ms)
     return s ? s : fail(h, MMNB_ERR_CUDA, cudaGetErrorString(ec));
   }
   cudaEvent_t a = nullptr, b = nullptr;
-  cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+  cudaError_t e = cudaGraphInstantiate(&ge, g, cudaGraphInstantiateFlagUseNodePriority);
   if (e == cudaSuccess)
     e = cudaEventCreate(&a);
   if (e == cudaSuccess)

@@ -456,7 +456,7 @@ static int md_capture(mmnb_md *md, double *log)
   }
   MDCK(ec);
   md->graph = g;
-  MDCK(cudaGraphInstantiate(&md->exec, g, 0));
+  MDCK(cudaGraphInstantiate(&md->exec, g, cudaGraphInstantiateFlagUseNodePriority));
   return MMNB_OK;
 }
 
@@ -630,7 +630,7 @@ static int batch_capture(mmnb_md_batch *b)
     return batch_fail(b, MMNB_ERR_CUDA, cudaGetErrorString(e != cudaSuccess ? e : ec));
   }
   b->graph = g;
-  e = cudaGraphInstantiate(&b->exec, g, 0);
+  e = cudaGraphInstantiate(&b->exec, g, cudaGraphInstantiateFlagUseNodePriority);
   if (e != cudaSuccess)
     return batch_fail(b, MMNB_ERR_CUDA, cudaGetErrorString(e));
   return MMNB_OK;

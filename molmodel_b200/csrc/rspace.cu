@@ -311,6 +311,7 @@ struct ExclArgs {
   Box box;
   double eta, e14, l14;
   int scale_e14, scale_l14, geometric, do14;
+  int assign;  // write the site arrays (first writer of the evaluation) instead of adding
   const double *r, *q, *sig, *eps, *rscreen;
   const int *mask, *excl_ptr, *excl_idx, *p14_ptr, *p14_idx;
   double *phi, *evec, *ljf;
@@ -402,14 +403,25 @@ __global__ void __launch_bounds__(kExclThreads) k_exclusions_fp64(ExclArgs a)
         }
       }
     }
-    a.phi[i] += phi;
-    a.evec[3 * i] += ex;
-    a.evec[3 * i + 1] += ey;
-    a.evec[3 * i + 2] += ez;
-    if (a.do14) {
-      a.ljf[3 * i] += lx;
-      a.ljf[3 * i + 1] += ly;
-      a.ljf[3 * i + 2] += lz;
+    if (a.assign) {
+      // the same bits as adding to zeroed arrays (0 + x, which also turns -0 into +0)
+      a.phi[i] = 0.0 + phi;
+      a.evec[3 * i] = 0.0 + ex;
+      a.evec[3 * i + 1] = 0.0 + ey;
+      a.evec[3 * i + 2] = 0.0 + ez;
+      a.ljf[3 * i] = 0.0 + lx;
+      a.ljf[3 * i + 1] = 0.0 + ly;
+      a.ljf[3 * i + 2] = 0.0 + lz;
+    } else {
+      a.phi[i] += phi;
+      a.evec[3 * i] += ex;
+      a.evec[3 * i + 1] += ey;
+      a.evec[3 * i + 2] += ez;
+      if (a.do14) {
+        a.ljf[3 * i] += lx;
+        a.ljf[3 * i + 1] += ly;
+        a.ljf[3 * i + 2] += lz;
+      }
     }
   }
   sl[threadIdx.x] = elj;
@@ -505,6 +517,9 @@ cudaError_t launch_exclusions(mmnb_handle *h, const double *d_r)
   a.scale_l14 = fabs(h->cfg.lj_1_4_scale_factor - 1) > 1e-10;
   a.geometric = h->cfg.geometric_combining_for_sigma;
   a.do14 = h->use_14 ? 1 : 0;
+  // the mixed form's pair kernels leave the FP64 site arrays alone: the
+  // exclusion corrections are their first write of an evaluation
+  a.assign = h->cfg.precision == MMNB_MIXED ? 1 : 0;
   a.r = d_r;
   a.q = h->d_q;
   a.sig = h->d_sig;
