@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison leg")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default launch choices instead of timing them (for launch-list captures)")
     return ap.parse_args()
 
 
@@ -228,7 +230,7 @@ def run_ours(args):
 
     main = make(args.precision)
     # launch choices that change no result, timed on this GPU (mmnb_autotune)
-    tuning = main.autotune(wb.positions, iters=10)
+    tuning = main.tuning if args.no_tune else main.autotune(wb.positions, iters=10)
     with ClockSampler(bus) as clk:
         total_ms, launches = timed_loop(main, args.steps, args.warmup, graph=True)
     t = torch.tensor([total_ms], dtype=torch.float64, device=dev)

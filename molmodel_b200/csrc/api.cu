@@ -955,10 +955,13 @@ int mmnb_graph_launch(mmnb_handle *h)
 }
 
 // f[i] += src[i] over [b, e), split over host threads when the range is large
+// f += src over [b, e) on the host cores: the add of each chunk runs while
+// the next chunk is in flight, and its memory traffic (two reads and a write
+// of the chunk) bounds the host call's tail
 static void add_forces(double *f, const double *src, size_t b, size_t e)
 {
   const long n = (long) (e - b);
-#pragma omp parallel for schedule(static) if (n > (1 << 16))
+#pragma omp parallel for schedule(static) if (n > (1 << 12))
   for (long i = 0; i < n; i++)
     f[b + i] += src[b + i];
 }

@@ -210,7 +210,7 @@ struct mmnb_handle {
   cudaGraphExec_t hgraph_exec = nullptr;
   long host_launch_per_eval = 0;
   // the host call copies the forces back in chunks and adds each as it lands
-  static constexpr int kChunks = 8;
+  static constexpr int kChunks = 4;
   cudaEvent_t ev_chunk[kChunks] = {};
   cudaEvent_t ev_flags = nullptr;
   bool capturing = false;
