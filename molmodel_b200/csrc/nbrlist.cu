@@ -304,9 +304,11 @@ __device__ __forceinline__ void build_row(const RebuildArgs &a, int p, int lane,
 #pragma unroll 4
     for (int t = lane; t < segn; t += 32) {
       const int s = g0 + t;
-      const int jx = (ix + a.stencil[3 * s]) % n;
-      const int jy = (iy + a.stencil[3 * s + 1]) % n;
-      const int jz = (iz + a.stencil[3 * s + 2]) % n;
+      // cell and stencil components are in [0, n): one conditional subtraction wraps
+      int jx = ix + a.stencil[3 * s], jy = iy + a.stencil[3 * s + 1], jz = iz + a.stencil[3 * s + 2];
+      jx -= jx >= n ? n : 0;
+      jy -= jy >= n ? n : 0;
+      jz -= jz >= n ? n : 0;
       const int rj = a.cell_rank[(jx * n + jy) * n + jz];
       ranges[t] = make_int2(a.start[rj], a.start[rj + 1]);
     }
