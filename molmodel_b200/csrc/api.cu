@@ -257,7 +257,10 @@ int alloc_rows(mmnb_handle *h, int cap)
 {
   drop_host_graph(h);
   h->rowcap = std::max(1, std::min(cap, h->ngroup));
-  return dalloc(h, &h->d_nbr, (size_t) h->ngroup * h->rowcap);
+  int s = dalloc(h, &h->d_nbr, (size_t) h->ngroup * h->rowcap);
+  if (!s && h->prune_margin > 0)
+    s = dalloc(h, &h->d_pnbr, (size_t) h->ngroup * h->rowcap);
+  return s;
 }
 
 int initial_rowcap(const mmnb_handle *h)
@@ -382,7 +385,8 @@ void free_all(mmnb_handle *h)
                   h->d_gexcl_idx, h->d_mask, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_cheb,
                   h->d_stencil, h->d_cell_rank, h->d_cell_of_rank, h->d_cell_of_group, h->d_cell_count,
                   h->d_cell_start, h->d_slot, h->d_sorted, h->d_rank, h->d_anchor, h->d_last, h->d_anchor_sorted, h->d_anchor32, h->d_block_sum,
-                  h->d_top2, h->d_nbr, h->d_nbr_count, h->d_flags, h->d_sr, h->d_sp, h->d_site_of_slot,
+                  h->d_top2, h->d_nbr, h->d_nbr_count, h->d_pnbr, h->d_pcount, h->d_plast, h->d_flags, h->d_sr,
+                  h->d_sp, h->d_site_of_slot,
                   h->d_phi, h->d_evec, h->d_ljf, h->d_lj_part, h->d_elec_part, h->d_energy, h->d_r, h->d_f,
                   h->d_mesh, h->d_meshk, h->d_green, h->d_kvec, h->d_egrid, h->d_egridk, h->d_mesh32,
                   h->d_meshk32, h->d_green32, h->d_mesh_fx, h->d_kint, h->d_kvecs, h->d_ak, h->d_skc,
@@ -656,7 +660,8 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
   CK(cudaMemset(h->d_flags, 0, sizeof(int) * kFlagCount));
   CK(cudaMallocHost((void **) &h->h_flags, sizeof(int) * kFlagCount));
   h->top2_blocks = std::min(256, div_up(ngroup, 256));
-  if ((s = dalloc(h, &h->d_top2, 2 * (size_t) h->top2_blocks)))
+  // per block: the two largest moves since the last build, then since the last prune
+  if ((s = dalloc(h, &h->d_top2, 4 * (size_t) h->top2_blocks)))
     return s;
   const size_t nslot = (size_t) ngroup * h->G;
   if ((s = dalloc(h, &h->d_sr, nslot)) || (s = dalloc(h, &h->d_sp, nslot)) ||
@@ -685,6 +690,13 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
   CK(cudaMallocHost((void **) &h->h_f, sizeof(double) * 3 * (size_t) nsite));
   CK(cudaMallocHost((void **) &h->h_out, sizeof(double) * 16));
   if ((s = setup_cells(h)))
+    return s;
+  // the rigid-water kernel's rows pruned to rc + width / 3: rebuilt (by that
+  // kernel, from the full rows) whenever the two largest anchor moves since
+  // the last prune exceed width / 3, so every pair within rc stays listed
+  h->prune_margin = (c->precision == MMNB_MIXED && h->nlw >= 0.3) ? h->nlw / 3 : 0.0;
+  if (h->prune_margin > 0 &&
+      ((s = dalloc(h, &h->d_pcount, ngroup)) || (s = dalloc(h, &h->d_plast, 3 * (size_t) ngroup))))
     return s;
   if ((s = alloc_rows(h, initial_rowcap(h))))
     return s;

@@ -22,7 +22,10 @@ enum FlagIndex {
   kFlagOverflow = 1,   // largest row length seen when a row overflowed
   kFlagError = 2,      // MMNB_ERR_DEVICE when a device-side check failed
   kFlagMaxRow = 3,     // largest row length of the last build
-  kFlagCount = 8
+  // 4: evaluations, 5: rebuilds, 6: the list check's block counter
+  kFlagPruneFull = 7,  // 1: the water kernel reads the full rows and writes the pruned ones
+  kFlagPruneValid = 8, // 1 while the pruned rows belong to the current build
+  kFlagCount = 10
 };
 
 // Box in the form the kernels use (cubic and orthorhombic).
@@ -140,6 +143,11 @@ struct mmnb_handle {
   int rowcap = 0;
   int *d_nbr = nullptr;              // ngroup * rowcap, sorted positions
   int *d_nbr_count = nullptr;        // ngroup
+  // rows pruned to rc + prune_margin for the rigid-water kernel (same rowcap),
+  // and the sorted anchors at the last prune
+  int *d_pnbr = nullptr, *d_pcount = nullptr;
+  double *d_plast = nullptr;
+  double prune_margin = 0;           // 0: no pruning
   int *d_flags = nullptr;            // mmnb::kFlagCount ints
   int *h_flags = nullptr;            // pinned mirror
   long rebuilds = 0, evals = 0;

@@ -70,6 +70,7 @@ __device__ __forceinline__ void block_top2(double &a, double &b, double *sa, dou
   }
   a = sa[0];
   b = sb[0];
+  __syncthreads();  // sa, sb may be reused at once
 }
 
 // Anchors of this evaluation, the two largest anchor moves since the last
@@ -78,17 +79,24 @@ __device__ __forceinline__ void block_top2(double &a, double &b, double *sa, dou
 // the last block to finish merges the block results.  On a rebuild the last
 // block also clears the cell counts for the rebuild kernel.
 // flags[4] counts evaluations, flags[5] rebuilds, flags[6] is the block counter.
+// With pruned rows (prune > 0; the rigid-water kernel) the same pass takes
+// the two largest moves since the last prune (plast, sorted order of the
+// build) and sets flags[kFlagPruneFull] when the pruned rows must be made
+// again: after a rebuild, while they are not valid, or when those moves add
+// up to more than the prune margin.
 __global__ void __launch_bounds__(kCheckThreads) k_list_check(const double *__restrict__ r,
                                                               const int *__restrict__ group, int ngroup,
                                                               const double *__restrict__ last, double width,
                                                               int first, int force, int interval,
                                                               double *__restrict__ anchor,
                                                               double *__restrict__ partial, int *__restrict__ flags,
-                                                              int *__restrict__ cell_count, int ncell3)
+                                                              int *__restrict__ cell_count, int ncell3,
+                                                              double prune, const int *__restrict__ rank,
+                                                              const double *__restrict__ plast)
 {
   __shared__ double sa[kCheckThreads], sb[kCheckThreads];
   __shared__ bool last_block;
-  double a = 0, b = 0;
+  double a = 0, b = 0, pa = 0, pb = 0;
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroup; g += gridDim.x * blockDim.x) {
     const int s0 = group[2 * g];
     const double x = r[3 * s0], y = r[3 * s0 + 1], z = r[3 * s0 + 2];
@@ -105,11 +113,26 @@ __global__ void __launch_bounds__(kCheckThreads) k_list_check(const double *__re
     } else if (d > b) {
       b = d;
     }
+    if (prune > 0) {
+      const int p = rank[g];
+      const double ex = x - plast[3 * p], ey = y - plast[3 * p + 1], ez = z - plast[3 * p + 2];
+      const double e = sqrt(ex * ex + ey * ey + ez * ez);
+      if (e > pa) {
+        pb = pa;
+        pa = e;
+      } else if (e > pb) {
+        pb = e;
+      }
+    }
   }
   block_top2(a, b, sa, sb);
+  if (prune > 0)
+    block_top2(pa, pb, sa, sb);
   if (threadIdx.x == 0) {
-    partial[2 * blockIdx.x] = a;
-    partial[2 * blockIdx.x + 1] = b;
+    partial[4 * blockIdx.x] = a;
+    partial[4 * blockIdx.x + 1] = b;
+    partial[4 * blockIdx.x + 2] = pa;
+    partial[4 * blockIdx.x + 3] = pb;
     __threadfence();
     last_block = atomicAdd(flags + 6, 1) == (int) gridDim.x - 1;
   }
@@ -117,10 +140,13 @@ __global__ void __launch_bounds__(kCheckThreads) k_list_check(const double *__re
   if (!last_block)
     return;
   __threadfence();
-  a = b = 0;
-  for (int i = threadIdx.x; i < (int) gridDim.x; i += blockDim.x)
-    top2_merge(a, b, partial[2 * i], partial[2 * i + 1]);
+  a = b = pa = pb = 0;
+  for (int i = threadIdx.x; i < (int) gridDim.x; i += blockDim.x) {
+    top2_merge(a, b, partial[4 * i], partial[4 * i + 1]);
+    top2_merge(pa, pb, partial[4 * i + 2], partial[4 * i + 3]);
+  }
   block_top2(a, b, sa, sb);
+  block_top2(pa, pb, sa, sb);
   __shared__ int rebuild_s;
   if (threadIdx.x == 0) {
     const int count = flags[4];
@@ -133,6 +159,9 @@ __global__ void __launch_bounds__(kCheckThreads) k_list_check(const double *__re
       flags[5] += 1;  // rebuild counter
     flags[6] = 0;
     rebuild_s = rebuild;
+    if (rebuild)
+      flags[kFlagPruneValid] = 0;
+    flags[kFlagPruneFull] = prune > 0 ? (rebuild || !flags[kFlagPruneValid] || pa + pb > prune) : 1;
   }
   __syncthreads();
   if (rebuild_s)
@@ -423,7 +452,8 @@ cudaError_t launch_list_check(mmnb_handle *h, const double *d_r, int force)
 {
   k_list_check<<<h->top2_blocks, kCheckThreads, 0, h->stream>>>(
       d_r, h->d_group, h->ngroup, h->d_last, h->nlw, h->first ? 1 : 0, force, h->cfg.rebuild_interval, h->d_anchor,
-      h->d_top2, h->d_flags, h->d_cell_count, h->ncell3);
+      h->d_top2, h->d_flags, h->d_cell_count, h->ncell3, h->water ? h->prune_margin : 0.0, h->d_rank,
+      h->d_plast);
   h->launches += 1;
   return cudaGetLastError();
 }

@@ -351,6 +351,12 @@ struct WaterArgs {
   const int *nbr, *nbr_count, *sorted, *group;
   long long *acc;         // per site: slots 4..6 receive the force, 0..3 are cleared
   unsigned long long *wsum;  // fixed-point Coulomb and LJ pair energies, zeroed by the prep kernel
+  // pruned rows (null: none): read when flags[kFlagPruneFull] is 0; made from
+  // the full rows (pairs with r^2 <= rp2) when it is 1
+  int *pnbr, *pcount;
+  double *plast;          // sorted anchors at the last prune
+  int *flags;
+  double rp2;
 };
 
 // One site pair of a water group pair: adds q_j b1 S d to the row site's field
@@ -444,8 +450,13 @@ __global__ void __launch_bounds__(kMxWarps * 32, MINB) k_pair_water(WaterArgs a)
     // the last product directly
     const float qO32 = qO * kTwo32, qH1_32 = h1.w * kTwo32, qH2_32 = h2.w * kTwo32;
     si0 = a.group[2 * a.sorted[p]];
-    const int cnt = a.nbr_count[p];
-    const int *row = a.nbr + (size_t) p * a.rowcap;
+    // full rows (and make the pruned ones), or the pruned rows
+    const bool make = a.pnbr && a.flags[kFlagPruneFull];
+    const bool use_pruned = a.pnbr && !make;
+    const int cnt = use_pruned ? a.pcount[p] : a.nbr_count[p];
+    const int *row = (use_pruned ? a.pnbr : a.nbr) + (size_t) p * a.rowcap;
+    int *prow = make ? a.pnbr + (size_t) p * a.rowcap : nullptr;
+    int pn = 0;
     const unsigned below = (1u << lane) - 1;
     auto compute = [&](int k) {
       const float4 da = qa[k], j1 = q1[k], j2 = q2[k];
@@ -517,6 +528,13 @@ __global__ void __launch_bounds__(kMxWarps * 32, MINB) k_pair_water(WaterArgs a)
       double x, y, z;
       const double r2a = anchor_disp_fast(a.box, ai, ac, x, y, z);
       const bool take = base + lane < cnt && r2a <= a.rhi2;
+      if (make) {
+        const bool keep = base + lane < cnt && r2a <= a.rp2;
+        const unsigned kb = __ballot_sync(0xffffffffu, keep);
+        if (keep)
+          prow[pn + __popc(kb & below)] = jc;
+        pn += __popc(kb);
+      }
       const unsigned bal = __ballot_sync(0xffffffffu, take);
       if (take) {
         const int slot = (head + qn + __popc(bal & below)) & kMask;
@@ -549,7 +567,15 @@ __global__ void __launch_bounds__(kMxWarps * 32, MINB) k_pair_water(WaterArgs a)
     for (; qn > 0; qn -= 32, head = (head + 32) & kMask)
       if (lane < qn)
         compute((head + lane) & kMask);
+    if (make && lane == 0) {
+      a.pcount[p] = pn;
+      a.plast[3 * p] = ai.x;
+      a.plast[3 * p + 1] = ai.y;
+      a.plast[3 * p + 2] = ai.z;
+    }
   }
+  if (a.pnbr && a.flags[kFlagPruneFull] && blockIdx.x == 0 && threadIdx.x == 0)
+    a.flags[kFlagPruneValid] = 1;
   __shared__ long long wsum[kMxWarps][2];
   // lane totals, transposed through the warp's own ring (no longer in use)
   static_assert(32 * (kCols + 1) * sizeof(long long) <= sizeof(ring[0]), "ring too small for the reduction");
@@ -609,6 +635,11 @@ cudaError_t launch_rspace_water(mmnb_handle *h)
   a.group = h->d_group;
   a.acc = h->mx.acc;
   a.wsum = h->d_wsum;
+  a.pnbr = h->prune_margin > 0 ? h->d_pnbr : nullptr;
+  a.pcount = h->d_pcount;
+  a.plast = h->d_plast;
+  a.flags = h->d_flags;
+  a.rp2 = (h->rc + h->prune_margin) * (h->rc + h->prune_margin);
   if (h->tune.water_minb == 5)
     k_pair_water<5><<<pair_blocks(h), kMxWarps * 32, 0, h->stream>>>(a);
   else
