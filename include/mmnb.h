@@ -265,6 +265,22 @@ int mmnb_set_tuning(mmnb_handle *h, const int tuning[3]);
 int mmnb_backward(mmnb_handle *h, const double *r, const double *dl_df, double *f, double *u,
                   double grad_u[3], double grad_l[3]);
 
+/* ---- potential at points ---------------------------------------------------
+   Electrostatic potential of the sites at r (3*nsite, host) at npoint points
+   (3*npoint, host), written to phi[npoint] in the units of mmnb_compute's phi
+   (the reference's internal potential unit; potential_unit_to_hartree_e,
+   include/units.h:106-109, converts it to atomic units for printing, as
+   ElecLJ::write_electrostatic_potential_at_gridpoints does).
+   Replaces ElecLJ::electrostatic_potential_at_gridpoints
+   (src/eleclj.cpp:1302-1340, periodic boxes): real space as
+   RSpaceEwaldPhiAtGridpoints (src/rspace.c:892-967, site-point distance cut at
+   rc and switched), the ordinary Ewald k-sum over kspace_cutoff wave vectors as
+   kspace_phi (src/kspace.c:176-250) whether or not the handle uses P3M for
+   forces, and the neutralising term when the sites carry net charge; each
+   term follows include_rspace / include_kspace / include_self.  Brute force over
+   sites x points, like the reference; allocates and frees its own scratch. */
+int mmnb_phi_at_points(mmnb_handle *h, const double *r, int npoint, const double *points, double *phi);
+
 /* ---- molecular dynamics on the device ------------------------------------
    Velocity Verlet with rigid 3-site water, replacing the MD loop of
    MDyn::run (src/mdyn.cpp:142-160: half kick, drift, constrain positions,

@@ -131,6 +131,19 @@ class ElecLJ:
             out.update(phi=phi, evec=evec)
         return out
 
+    def electrostatic_potential_at_gridpoints(self, r, points):
+        """ElecLJ::electrostatic_potential_at_gridpoints (src/eleclj.cpp:1302-1340):
+        potential of the sites at r (nsite x 3) at each point (npoint x 3), in
+        the units of compute()'s phi; real space, the kspace_cutoff k-sum and
+        the neutralising term, each as include_rspace / include_kspace /
+        include_self say."""
+        lib = load()
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+        phi = np.zeros(len(pts))
+        check(lib.mmnb_phi_at_points(self._h, _d(r), len(pts), _d(pts), _d(phi)), self._h)
+        return phi
+
     def add_to_energy_and_forces(self, u, f, r):
         """Potential::add_to_energy_and_forces: forces are added to ``f``
         (nsite x 3, float64, in place); returns ``u`` plus the energy."""

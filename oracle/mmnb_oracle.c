@@ -1435,6 +1435,80 @@ int orc_eleclj_eval(void *hp, const double *r, double *f, orc_energy *e,
   return 0;
 }
 
+/* Potential at points (ElecLJ::electrostatic_potential_at_gridpoints,
+   src/eleclj.cpp:1302-1340, periodic branch).  Real space as
+   RSpaceEwaldPhiAtGridpoints (src/rspace.c:892-967): site minus point, minimum
+   image, cut and switched on that distance, the site's own r_screen; k-space as
+   kspace_phi (src/kspace.c:176-250) over points and sites with the points
+   uncharged; the neutralising term for a charged system. */
+int orc_eleclj_phi_at_points(void *hp, const double *r, int npoint, const double *pts, double *phi_out)
+{
+  elec_t *h = (elec_t *) hp;
+  const int n = h->nsite, ntot = npoint + n;
+  const double rlo2 = sq(h->rc - h->c.smoothing_width), rhi2 = sq(h->rc);
+  double *p = (double *) calloc(ntot > 0 ? ntot : 1, sizeof(double));
+  int i, j, d;
+  if (h->c.include_rspace && h->cheb) {
+    for (i = 0; i < n; i++) {
+      if (!h->mask[i])
+        continue;
+      for (j = 0; j < npoint; j++) {
+        double v[3], dv[3], r2, b0, b1;
+        for (d = 0; d < 3; d++)
+          v[d] = r[3 * i + d] - pts[3 * j + d];
+        image_shift(&h->box, v, dv);
+        for (d = 0; d < 3; d++)
+          v[d] += dv[d];
+        r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        if (r2 > rhi2)
+          continue;
+        if (h->cheb->min < r2 && r2 < h->cheb->max) {
+          cheb_eval(h->cheb, r2, &b0, &b1);
+        } else {
+          const double rm = sqrt(r2);
+          b0 = erfc(h->eta * rm) / rm;
+        }
+        if (r2 < sq(h->rscreen[i])) {
+          const double rs = h->rscreen[i];
+          b0 += (-0.5 * r2 * (1.0 / (rs * rs * rs)) + 1.5 / rs) - 1.0 / sqrt(r2);
+        }
+        if (r2 > rlo2) {
+          const double z = (r2 - rlo2) / (rhi2 - rlo2);
+          b0 *= ((-6 * z + 15) * z - 10) * z * z * z + 1;
+        }
+        p[j] += h->q[i] * b0;
+      }
+    }
+  }
+  if (h->c.include_kspace) {
+    double rec[9];
+    double *rt = (double *) malloc(sizeof(double) * 3 * (ntot > 0 ? ntot : 1));
+    double *qt = (double *) calloc(ntot > 0 ? ntot : 1, sizeof(double));
+    double *et = (double *) calloc(3 * (ntot > 0 ? ntot : 1), sizeof(double));
+    memcpy(rt, pts, sizeof(double) * 3 * npoint);
+    memcpy(rt + 3 * npoint, r, sizeof(double) * 3 * n);
+    memcpy(qt + npoint, h->q, sizeof(double) * n);
+    t_reciprocal(rec, h->latv);
+    kspace_sum(h->c.kspace_cutoff, ntot, rt, qt, rec, box_volume(&h->box), h->eta, p, et);
+    free(rt);
+    free(qt);
+    free(et);
+  }
+  if (h->c.include_self) {
+    double qs = 0;
+    for (i = 0; i < n; i++)
+      qs += h->q[i];
+    if (!almost_zero(qs)) {
+      const double b = -M_PI / (sq(h->eta) * box_volume(&h->box)) * qs;
+      for (j = 0; j < npoint; j++)
+        p[j] += b;
+    }
+  }
+  memcpy(phi_out, p, sizeof(double) * npoint);
+  free(p);
+  return 0;
+}
+
 double orc_eleclj_eta(void *hp) { return ((elec_t *) hp)->eta; }
 double orc_eleclj_nlw(void *hp) { return ((elec_t *) hp)->nlw; }
 void *orc_eleclj_nbrlist(void *hp) { return ((elec_t *) hp)->nl; }

@@ -130,6 +130,7 @@ class OracleLib:
         L.orc_eleclj_nlw.argtypes = [_vp]
         L.orc_eleclj_nbrlist.restype = _vp
         L.orc_eleclj_nbrlist.argtypes = [_vp]
+        L.orc_eleclj_phi_at_points.argtypes = [_vp, _dp, ctypes.c_int, _dp, _dp]
         L.orc_eleclj_delete.argtypes = [_vp]
         L.orc_pairset_demo.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _ip, _ip]
 
@@ -238,6 +239,13 @@ class ElecLJ:
         self.L.lib.orc_eleclj_eval(self.h, _d(r), _d(f), ctypes.byref(e), _d(phi), _d(evec), _d(ljf))
         return dict(f=f, phi=phi, evec=evec, ljf=ljf, elec=e.elec, lj=e.lj,
                     lj_correction=e.lj_correction, total=e.total)
+
+    def phi_at_points(self, r, points):
+        """Potential of the sites at r at the points (ElecLJ::electrostatic_potential_at_gridpoints)."""
+        r, pts = _f64(r), _f64(points).reshape(-1, 3)
+        phi = np.zeros(len(pts))
+        self.L.lib.orc_eleclj_phi_at_points(self.h, _d(r), len(pts), _d(pts), _d(phi))
+        return phi
 
     @property
     def eta(self):

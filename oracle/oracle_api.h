@@ -94,6 +94,10 @@ int orc_eleclj_eval(void *h, const double *r, double *f, orc_energy *e,
 double orc_eleclj_eta(void *h);
 double orc_eleclj_nlw(void *h);
 void *orc_eleclj_nbrlist(void *h);
+/* Electrostatic potential of the sites at r at npoint points (3*npoint), written
+   to phi[npoint] (ElecLJ::electrostatic_potential_at_gridpoints,
+   src/eleclj.cpp:1302-1340, periodic branch). */
+int orc_eleclj_phi_at_points(void *h, const double *r, int npoint, const double *pts, double *phi);
 void orc_eleclj_delete(void *h);
 
 /* Pair-set semantics (src/pbin.c:41-137): add the 2*nadd pairs in order, sort

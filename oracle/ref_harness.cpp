@@ -468,6 +468,45 @@ int orc_eleclj_eval(void *hp, const double *r, double *f, orc_energy *e,
   return 0;
 }
 
+/* ElecLJ::electrostatic_potential_at_gridpoints, periodic branch
+   (src/eleclj.cpp:1302-1340), with the reference's own RSpaceEwaldPhiAtGridpoints
+   and kspace_new/kspace_phi over points + sites (the points carry no charge). */
+int orc_eleclj_phi_at_points(void *hp, const double *r, int npoint, const double *pts, double *phi_out)
+{
+  RefElecLJ *h = (RefElecLJ *) hp;
+  const orc_config &c = h->c;
+  const int nsite = h->nsite, ntot = npoint + nsite;
+  std::vector<double> p(ntot, 0.0);
+  if (c.include_rspace)
+    RSpaceEwaldPhiAtGridpoints(nsite, npoint, (const cart_t *) r, (const cart_t *) pts, h->bc->type,
+                               (const tensor_t *) &h->latv, sqr(h->rc - c.smoothing_width), sqr(h->rc),
+                               h->site_mask.data(), h->q.data(), p.data(), h->eta, h->cheb, h->rscreen.data());
+  if (c.include_kspace) {
+    std::vector<double> qtot(ntot, 0.0), rtot(3 * (size_t) ntot);
+    memcpy(rtot.data(), pts, sizeof(double) * 3 * npoint);
+    memcpy(rtot.data() + 3 * (size_t) npoint, r, sizeof(double) * 3 * nsite);
+    for (int i = 0; i < nsite; i++)
+      qtot[npoint + i] = h->q[i];
+    struct kspace *ks = kspace_new(c.kspace_cutoff, ntot);
+    const Tensor recip = h->bc->reciprocal_lattice_vectors();
+    kspace_phi(ks, (const cart_t *) rtot.data(), qtot.data(), (const tensor_t *) &recip, h->bc->volume(), h->eta,
+               p.data());
+    kspace_delete(ks);
+  }
+  if (c.include_self) {
+    double qsum = 0;
+    for (int i = 0; i < nsite; i++)
+      qsum += h->q[i];
+    if (!is_almost_zero(qsum)) {
+      const double b = -M_PI / (sqr(h->eta) * h->bc->volume()) * qsum;
+      for (int i = 0; i < npoint; i++)
+        p[i] += b;
+    }
+  }
+  memcpy(phi_out, p.data(), sizeof(double) * npoint);
+  return 0;
+}
+
 double orc_eleclj_eta(void *hp) { return ((RefElecLJ *) hp)->eta; }
 double orc_eleclj_nlw(void *hp) { return ((RefElecLJ *) hp)->nlw; }
 void *orc_eleclj_nbrlist(void *hp) { return &((RefElecLJ *) hp)->nbr; }

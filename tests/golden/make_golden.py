@@ -75,6 +75,38 @@ def pbin_kat(reference_root):
     return dict(source="src/pbin.c:152-214", n=n, adds=adds, rows=[rows[i] for i in range(n)], exists=matrix)
 
 
+def esp_fixture(ref):
+    """Potential at points (ElecLJ::electrostatic_potential_at_gridpoints): a
+    neutral box with the k-sum, and a charged box with screening radii whose
+    forces use P3M (the potential at points still uses the k-sum)."""
+    rng = np.random.default_rng(11)
+    out = {}
+    for tag, n, seed, cfg, charged in (("ksum", 6, 1, C1, False), ("p3m", 5, 3, P3M_SMALL, True)):
+        wb = water_box(n, seed=seed)
+        q = wb.q.copy()
+        rscreen = wb.rscreen.copy()
+        if charged:
+            q[0] += 0.2 * q[1]
+            rscreen = np.where(np.arange(wb.nsite) % 3 == 0, 1.6, 0.0)
+        # points anywhere in (and slightly outside) the box, and points 0.4-2.5 A
+        # from sites (closed-form erfc below r = 2 A, the screening radius, the table)
+        far = rng.uniform(-0.1 * wb.box, 1.1 * wb.box, size=(96, 3))
+        k = rng.choice(wb.nsite, size=96, replace=False)
+        d = rng.normal(size=(96, 3))
+        d *= (rng.uniform(0.4, 2.5, size=96) / np.linalg.norm(d, axis=1))[:, None]
+        pts = np.concatenate([far, wb.positions[k] + d])
+        o = ref.eleclj(make_config(wb.box, **cfg), wb.nsite, wb.groups, wb.exclusions, wb.site_mask, q,
+                       wb.sigma, wb.epsilon, rscreen)
+        out[tag + "_n"] = n
+        out[tag + "_seed"] = seed
+        out[tag + "_config"] = json.dumps(cfg)
+        out[tag + "_q"] = q
+        out[tag + "_rscreen"] = rscreen
+        out[tag + "_points"] = pts
+        out[tag + "_phi"] = o.phi_at_points(wb.positions, pts)
+    np.savez_compressed(os.path.join(HERE, "esp_points.npz"), **out)
+
+
 def main():
     reference_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     ref = reference()
@@ -101,6 +133,7 @@ def main():
          exclusions=excl, rscreen=rscreen, pairs14=p14)
     mn, mx, inv, coeff = ref.chebyshev(9.0, 0.35)
     np.savez_compressed(os.path.join(HERE, "cheb_9_0.35.npz"), min=mn, max=mx, inv_dx=inv, coeff=coeff)
+    esp_fixture(ref)
     print("golden fixtures written to", HERE)
 
 

@@ -132,3 +132,15 @@ def test_port_vs_reference_kspace_field():
     pb, eb, nb = port().kspace_field(6.0, wb.positions, wb.q, latv, 0.4)
     assert na == nb
     assert rel_max(pb, pa) < 1e-12 and rel_max(eb, ea) < 1e-12
+
+
+@pytest.mark.parametrize("tag", ["ksum", "p3m"])
+def test_golden_phi_at_points(tag):
+    """The restatement of ElecLJ::electrostatic_potential_at_gridpoints against
+    the reference's own RSpaceEwaldPhiAtGridpoints + kspace_phi (fixture)."""
+    g = load("esp_points.npz")
+    wb = water_box(int(g[tag + "_n"]), seed=int(g[tag + "_seed"]))
+    cfg = json.loads(str(g[tag + "_config"]))
+    o, _ = run(port(), wb, cfg, q=g[tag + "_q"], rscreen=g[tag + "_rscreen"])
+    phi = o.phi_at_points(wb.positions, g[tag + "_points"])
+    assert rel_max(phi, g[tag + "_phi"]) < 1e-12
