@@ -280,7 +280,7 @@ def run_ours(args):
            "config": {"workload": WORKLOAD, "precision": args.precision, "l2": "flushed (256 MB write) before every "
                       "timed step", "parallelism": f"replicas x{world}", "dt_fs_for_ns_per_day": DT_FS,
                       "launch": "CUDA graph of one evaluation, replayed per step",
-                      "tuning": {"water_kernel_blocks_per_sm": tuning[0], "spread_layout":
+                      "tuning": {"water_kernel_registers": 128 if tuning[0] == 4 else 96, "spread_layout":
                                  ("thread per site", "thread per site and x-plane",
                                   "lane per site and z-offset")[tuning[1]], "p3m_side_stream": bool(tuning[2])}},
            "ms_per_step_without_graph": nograph_ms / args.steps,

@@ -235,8 +235,9 @@ int mmnb_measure_fp32_peak(int device, double *tflops);
 
 /* ---- launch tuning ---------------------------------------------------------
    No counterpart in the reference (its path is one CPU thread).  Launch
-   choices that change no result: tuning[0] = resident blocks per SM of the
-   rigid-water pair kernel (4 or 5: its register budget), tuning[1] = layout
+   choices that change no result: tuning[0] = register budget of the
+   rigid-water pair kernel as resident warps per SM / 4 (4: 128 registers,
+   5: 96), tuning[1] = layout
    of the mixed P3M charge assignment (0: a thread per site, 1: a thread per
    site and mesh x-plane, 2 (default): a lane per site and mesh z-offset, so
    the lanes of a site reduce into consecutive mesh words),

@@ -339,6 +339,11 @@ __global__ void __launch_bounds__(kMxWarps * 32) k_pair_mixed(MixedArgs a)
 // values to fixed point.
 
 constexpr int kWaterRing = 128;
+// Warps (rows) per block of the rigid-water kernel: one, so a block retires as
+// soon as its row is done and its slot takes the next row (rows differ in
+// length; with four warps per block the finished warps idle until the block's
+// longest row ends)
+constexpr int kWaterWarps = 1;
 
 struct WaterArgs {
   int ngroup, rowcap, geometric;
@@ -420,15 +425,15 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// MINB: resident blocks per SM the register budget is cut for (4: 128
+// MINB: resident warps per SM / 4 the register budget is cut for (4: 128
 // registers, 5: 96); mmnb_autotune picks per handle
 template <int MINB>
-__global__ void __launch_bounds__(kMxWarps * 32, MINB) k_pair_water(WaterArgs a)
+__global__ void __launch_bounds__(kWaterWarps * 32, MINB * kMxWarps / kWaterWarps) k_pair_water(WaterArgs a)
 {
   // per warp: ring of anchor displacement (xyz, r^2), partner O slot (zero
   // offset, charge), H1 and H2 slots (offset, charge); LJ parameters apart
-  __shared__ float4 ring[kMxWarps][4][kWaterRing];
-  __shared__ float2 ql[kMxWarps][kWaterRing];   // partner sigma, sqrt(eps)
+  __shared__ float4 ring[kWaterWarps][4][kWaterRing];
+  __shared__ float2 ql[kWaterWarps][kWaterRing];   // partner sigma, sqrt(eps)
   constexpr int kCols = 11;
   constexpr int kMask = kWaterRing - 1;
   constexpr float kTwo32 = 4294967296.0f, kTwo31 = 2147483648.0f;
@@ -437,7 +442,7 @@ __global__ void __launch_bounds__(kMxWarps * 32, MINB) k_pair_water(WaterArgs a)
   for (int c = 0; c < kCols; c++)
     fx[c] = 0;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int p = blockIdx.x * kMxWarps + w;
+  const int p = blockIdx.x * kWaterWarps + w;
   float4 *qa = ring[w][0], *q0 = ring[w][1], *q1 = ring[w][2], *q2 = ring[w][3];
   int si0 = 0;
   if (p < a.ngroup) {
@@ -576,7 +581,7 @@ __global__ void __launch_bounds__(kMxWarps * 32, MINB) k_pair_water(WaterArgs a)
   }
   if (a.pnbr && a.flags[kFlagPruneFull] && blockIdx.x == 0 && threadIdx.x == 0)
     a.flags[kFlagPruneValid] = 1;
-  __shared__ long long wsum[kMxWarps][2];
+  __shared__ long long wsum[kWaterWarps][2];
   // lane totals, transposed through the warp's own ring (no longer in use)
   static_assert(32 * (kCols + 1) * sizeof(long long) <= sizeof(ring[0]), "ring too small for the reduction");
   long long(*red)[kCols + 1] = reinterpret_cast<long long(*)[kCols + 1]>(ring[w]);
@@ -603,7 +608,7 @@ __global__ void __launch_bounds__(kMxWarps * 32, MINB) k_pair_water(WaterArgs a)
   __syncthreads();
   if (threadIdx.x == 0) {
     long long te = 0, tl = 0;
-    for (int k = 0; k < kMxWarps; k++) {
+    for (int k = 0; k < kWaterWarps; k++) {
       te += wsum[k][0];
       tl += wsum[k][1];
     }
@@ -640,10 +645,11 @@ cudaError_t launch_rspace_water(mmnb_handle *h)
   a.plast = h->d_plast;
   a.flags = h->d_flags;
   a.rp2 = (h->rc + h->prune_margin) * (h->rc + h->prune_margin);
+  const int blocks = div_up(h->ngroup, kWaterWarps);
   if (h->tune.water_minb == 5)
-    k_pair_water<5><<<pair_blocks(h), kMxWarps * 32, 0, h->stream>>>(a);
+    k_pair_water<5><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
   else
-    k_pair_water<4><<<pair_blocks(h), kMxWarps * 32, 0, h->stream>>>(a);
+    k_pair_water<4><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
   h->launches += 1;
   return cudaGetLastError();
 }

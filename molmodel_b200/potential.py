@@ -159,7 +159,7 @@ class ElecLJ:
 
     def autotune(self, r, iters=10):
         """Time the launch choices at positions r and keep the fastest;
-        returns them (water-kernel blocks per SM, spread layout, P3M stream)."""
+        returns them (water-kernel register budget code, spread layout, P3M stream)."""
         r = np.ascontiguousarray(r, dtype=np.float64)
         check(load().mmnb_autotune(self._h, _d(r), int(iters)), self._h)
         return self.tuning
