@@ -15,6 +15,7 @@ constexpr int kFinThreads = 256;
 
 struct FinArgs {
   int nsite, do_self;
+  int keep_fields;       // write phi, E and the LJ force back (the caller asked for the site fields)
   double self_a, neutral_b;
   const double *q;
   const long long *acc;  // mixed form: fixed-point potential, field and LJ force per site
@@ -52,9 +53,17 @@ __global__ void __launch_bounds__(kFinThreads) k_finalize(FinArgs a)
   if (i < a.nsite) {
     const double qi = a.q[i];
     double p = a.phi[i];
+    double ev[3], lf[3];
+    for (int d = 0; d < 3; d++) {
+      ev[d] = a.evec[3 * i + d];
+      lf[d] = a.ljf[3 * i + d];
+    }
     if (a.acc) {
-      // fold the fixed-point sums into the FP64 site arrays
-      const long long *o = a.acc + (size_t) i * kAccStride;
+      // fold the fixed-point sums into the FP64 site values (one site's words
+      // are 64 contiguous bytes: four 16-byte loads)
+      const longlong2 *o2 = reinterpret_cast<const longlong2 *>(a.acc + (size_t) i * kAccStride);
+      const longlong2 w01 = o2[0], w23 = o2[1], w45 = o2[2], w67 = o2[3];
+      const long long o[7] = {w01.x, w01.y, w23.x, w23.y, w45.x, w45.y, w67.x};
       long long k[4] = {0, 0, 0, 0};
       if (a.acck) {
         const longlong4 v = reinterpret_cast<const longlong4 *>(a.acck)[i];
@@ -65,20 +74,26 @@ __global__ void __launch_bounds__(kFinThreads) k_finalize(FinArgs a)
       }
       p += (double) (o[0] + k[0]) * kFxInv;
       for (int d = 0; d < 3; d++) {
-        a.evec[3 * i + d] += (double) (o[1 + d] + k[1 + d]) * kFxInv;
-        a.ljf[3 * i + d] += (double) o[4 + d] * kFxInv;
+        ev[d] += (double) (o[1 + d] + k[1 + d]) * kFxInv;
+        lf[d] += (double) o[4 + d] * kFxInv;
       }
     }
     if (a.do_self) {
       p -= a.self_a * qi;
       p += a.neutral_b;
     }
-    a.phi[i] = p;
     e = qi * p;
+    if (a.keep_fields) {
+      a.phi[i] = p;
+      for (int d = 0; d < 3; d++) {
+        a.evec[3 * i + d] = ev[d];
+        a.ljf[3 * i + d] = lf[d];
+      }
+    }
     if (a.f) {
-      a.f[3 * i] += qi * a.evec[3 * i] + a.ljf[3 * i];
-      a.f[3 * i + 1] += qi * a.evec[3 * i + 1] + a.ljf[3 * i + 1];
-      a.f[3 * i + 2] += qi * a.evec[3 * i + 2] + a.ljf[3 * i + 2];
+      a.f[3 * i] += qi * ev[0] + lf[0];
+      a.f[3 * i + 1] += qi * ev[1] + lf[1];
+      a.f[3 * i + 2] += qi * ev[2] + lf[2];
     }
   }
   const double bs = block_sum(e, se);
@@ -119,6 +134,7 @@ cudaError_t launch_finalize(mmnb_handle *h, double *d_f, double *d_energy)
   FinArgs a;
   a.nsite = h->nsite;
   a.do_self = (h->any_q && h->cfg.include_self) ? 1 : 0;
+  a.keep_fields = h->want_fields ? 1 : 0;
   a.self_a = h->eta * M_2_SQRTPI;
   // neutralising background for a charged system (src/eleclj.cpp:965-975)
   a.neutral_b = h->neutral_b;
