@@ -187,6 +187,9 @@ struct RebuildArgs {
   float4 *anchor32;
   float Lf[3], invLf[3];
   float c2lo, c2hi;
+  // per-row cull of stencil cells: a cell whose every point is farther than
+  // sqrt(c2cull) > cutoff + width from the row's anchor holds no partner
+  float lcf[3], c2cull;
   int *block_sum;            // per block of the launch: its segment's cell count
   int *scatter;              // groups by cell before the in-cell ordering (ngroup)
 };
@@ -338,8 +341,18 @@ __device__ __forceinline__ void build_row(const RebuildArgs &a, int p, int lane,
       jx -= jx >= n ? n : 0;
       jy -= jy >= n ? n : 0;
       jz -= jz >= n ? n : 0;
-      const int rj = a.cell_rank[(jx * n + jy) * n + jz];
-      ranges[t] = make_int2(a.start[rj], a.start[rj + 1]);
+      // lower bound of the distance from this row's anchor (wrapped into the
+      // box) to the cell's slab [c l - l/2, c l + l/2] on each axis, minimum image
+      float dx = wi.x - (float) jx * a.lcf[0], dy = wi.y - (float) jy * a.lcf[1], dz = wi.z - (float) jz * a.lcf[2];
+      dx = fmaxf(fabsf(dx - a.Lf[0] * rintf(dx * a.invLf[0])) - 0.5f * a.lcf[0], 0.f);
+      dy = fmaxf(fabsf(dy - a.Lf[1] * rintf(dy * a.invLf[1])) - 0.5f * a.lcf[1], 0.f);
+      dz = fmaxf(fabsf(dz - a.Lf[2] * rintf(dz * a.invLf[2])) - 0.5f * a.lcf[2], 0.f);
+      int2 rg = make_int2(0, 0);
+      if (s == 0 || dx * dx + dy * dy + dz * dz <= a.c2cull) {
+        const int rj = a.cell_rank[(jx * n + jy) * n + jz];
+        rg = make_int2(a.start[rj], a.start[rj + 1]);
+      }
+      ranges[t] = rg;
     }
     __syncwarp();
     for (int b0 = 0; b0 < segn; b0 += 32) {
@@ -513,6 +526,13 @@ cudaError_t launch_list_rebuild(mmnb_handle *h)
   const bool safe = std::sqrt(c2) + 1.0 < 0.45 * lmin;
   a.c2lo = safe ? (float) (c2 - tol) : -1.0f;
   a.c2hi = safe ? (float) (c2 + tol) : 3.0e38f;
+  // the cull keeps a 0.01 A margin over the FP32 rounding of the anchors and
+  // cell centres (~1e-5 A here); boxes where the FP32 minimum image is not
+  // safe keep every stencil cell
+  for (int d = 0; d < 3; d++)
+    a.lcf[d] = (float) h->cg.lc[d];
+  const double cull = std::sqrt(c2) + 0.01;
+  a.c2cull = safe ? (float) (cull * cull) : 3.0e38f;
   void *args[] = {&a};
   h->launches += 1;
   return cudaLaunchCooperativeKernel((const void *) k_list_rebuild, dim3(h->rebuild_grid), dim3(kRebuildThreads),
