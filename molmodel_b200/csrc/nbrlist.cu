@@ -331,34 +331,45 @@ __device__ __forceinline__ void build_row(const RebuildArgs &a, int p, int lane,
   int count = 0;
   for (int g0 = 0; g0 < a.nstencil; g0 += kSeg) {
     // the member ranges of a segment of stencil cells, fetched with independent
-    // loads (one dependent chain per cell instead of one per batch of 32)
+    // loads (one dependent chain per cell instead of one per batch of 32);
+    // the cells that can hold a partner and are not empty are compacted in
+    // stencil order, so the batches below see only them (the own cell, stencil
+    // entry 0, always has the row's group and comes first)
     const int segn = min(kSeg, a.nstencil - g0);
-#pragma unroll 4
-    for (int t = lane; t < segn; t += 32) {
-      const int s = g0 + t;
-      // cell and stencil components are in [0, n): one conditional subtraction wraps
-      int jx = ix + a.stencil[3 * s], jy = iy + a.stencil[3 * s + 1], jz = iz + a.stencil[3 * s + 2];
-      jx -= jx >= n ? n : 0;
-      jy -= jy >= n ? n : 0;
-      jz -= jz >= n ? n : 0;
-      // lower bound of the distance from this row's anchor (wrapped into the
-      // box) to the cell's slab [c l - l/2, c l + l/2] on each axis, minimum image
-      float dx = wi.x - (float) jx * a.lcf[0], dy = wi.y - (float) jy * a.lcf[1], dz = wi.z - (float) jz * a.lcf[2];
-      dx = fmaxf(fabsf(dx - a.Lf[0] * rintf(dx * a.invLf[0])) - 0.5f * a.lcf[0], 0.f);
-      dy = fmaxf(fabsf(dy - a.Lf[1] * rintf(dy * a.invLf[1])) - 0.5f * a.lcf[1], 0.f);
-      dz = fmaxf(fabsf(dz - a.Lf[2] * rintf(dz * a.invLf[2])) - 0.5f * a.lcf[2], 0.f);
+    int kept = 0;
+#pragma unroll 2
+    for (int t0 = 0; t0 < segn; t0 += 32) {
+      const int t = t0 + lane;
       int2 rg = make_int2(0, 0);
-      if (s == 0 || dx * dx + dy * dy + dz * dz <= a.c2cull) {
-        const int rj = a.cell_rank[(jx * n + jy) * n + jz];
-        rg = make_int2(a.start[rj], a.start[rj + 1]);
+      if (t < segn) {
+        const int s = g0 + t;
+        // cell and stencil components are in [0, n): one conditional subtraction wraps
+        int jx = ix + a.stencil[3 * s], jy = iy + a.stencil[3 * s + 1], jz = iz + a.stencil[3 * s + 2];
+        jx -= jx >= n ? n : 0;
+        jy -= jy >= n ? n : 0;
+        jz -= jz >= n ? n : 0;
+        // lower bound of the distance from this row's anchor (wrapped into the
+        // box) to the cell's slab [c l - l/2, c l + l/2] on each axis, minimum image
+        float dx = wi.x - (float) jx * a.lcf[0], dy = wi.y - (float) jy * a.lcf[1], dz = wi.z - (float) jz * a.lcf[2];
+        dx = fmaxf(fabsf(dx - a.Lf[0] * rintf(dx * a.invLf[0])) - 0.5f * a.lcf[0], 0.f);
+        dy = fmaxf(fabsf(dy - a.Lf[1] * rintf(dy * a.invLf[1])) - 0.5f * a.lcf[1], 0.f);
+        dz = fmaxf(fabsf(dz - a.Lf[2] * rintf(dz * a.invLf[2])) - 0.5f * a.lcf[2], 0.f);
+        if (s == 0 || dx * dx + dy * dy + dz * dz <= a.c2cull) {
+          const int rj = a.cell_rank[(jx * n + jy) * n + jz];
+          rg = make_int2(a.start[rj], a.start[rj + 1]);
+        }
       }
-      ranges[t] = rg;
+      const bool keep = rg.y > rg.x;
+      const unsigned kb = __ballot_sync(0xffffffffu, keep);
+      if (keep)
+        ranges[kept + __popc(kb & below)] = rg;
+      kept += __popc(kb);
     }
     __syncwarp();
-    for (int b0 = 0; b0 < segn; b0 += 32) {
+    for (int b0 = 0; b0 < kept; b0 += 32) {
       const int s0 = g0 + b0;
       int beg = 0, end = 0;
-      if (b0 + lane < segn) {
+      if (b0 + lane < kept) {
         const int2 rg = ranges[b0 + lane];
         beg = rg.x;
         end = rg.y;
