@@ -180,6 +180,8 @@ extern "C" int mmnb_phi_at_points(mmnb_handle *h, const double *r, int npoint, c
 {
   if (!h || !r || (npoint > 0 && (!points || !phi)) || npoint < 0)
     return esp_fail(h, MMNB_ERR_ARG, "null handle, positions, points or output, or a negative point count");
+  if (npoint > (1 << 30) / 3)
+    return esp_fail(h, MMNB_ERR_ARG, "at most 357,913,941 points per call (32-bit point indices)");
   if (!h->params_set)
     return esp_fail(h, MMNB_ERR_STATE, "mmnb_set_params has not been called");
   if (npoint == 0)
