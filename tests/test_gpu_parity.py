@@ -220,3 +220,33 @@ def test_energy_conservation_fd(c1):
     fd = -(ep - em) / (2 * h)
     an = float((g["f"] * d).sum())
     assert abs(fd - an) < 1e-6 * max(1.0, abs(an))
+
+
+def test_orthorhombic_list_with_cell_cull():
+    """A box large enough that the list build skips stencil cells per row
+    (different cell edges on the three axes, molecules also outside the box):
+    the pair list is still exactly the reference's, before and after a rebuild."""
+    wb = water_box(13, seed=21)
+    stretch = np.array([1.0, 1.12, 0.9])
+    r = wb.positions * stretch
+    r[0:30] += np.array([1.0, -2.0, 1.0]) * (wb.box * stretch)   # ten molecules one image away
+    box = wb.box * stretch
+
+    class Ortho:
+        pass
+    s = Ortho()
+    for k in ("nsite", "groups", "exclusions", "site_mask", "q", "sigma", "epsilon", "rscreen"):
+        setattr(s, k, getattr(wb, k))
+    s.box = box
+    cfg = dict(rspace_cutoff=9.0, ewald_screening=0.35, neighbor_list_width=1.5, use_p3m=True,
+               p3m_grid_spacing=1.2, p3m_assignment_order=4)
+    p = gpu_for(s, cfg, bctype=2)
+    o = oracle_for(port(), s, cfg, bctype=2, box=box)
+    rng = np.random.default_rng(4)
+    for step in range(3):
+        g = p.compute(r, want_fields=True)
+        oo = o.eval(r)
+        assert_parity(g, oo)
+        assert np.array_equal(canon_pairs(p.pairlist()), canon_pairs(o.nbrlist().pairs())), step
+        # whole molecules moved past the skin: the next evaluation rebuilds
+        r = (r.reshape(-1, 3, 3) + rng.normal(scale=0.2, size=(wb.nwater, 1, 3))).reshape(-1, 3)
