@@ -352,17 +352,21 @@ def read_profile_traffic(precision):
 # --------------------------------------------------------------------------- CPU legs
 def _ref_worker(conn, seed, n_warm, n_eval):
     """One process: build the reference's ElecLJ path on the workload, run
-    n_warm untimed evaluations (the first builds the neighbour list), then time
-    n_eval evaluations."""
+    n_warm untimed evaluations (the first builds the neighbour list), then,
+    on the coordinator's signals, time n_eval evaluations and then one
+    neighbour-list rebuild (the reference's NeighborList::rebuild_periodic over
+    the same anchors, on a list whose cells and stencil were set up untimed)."""
     sys.path.insert(0, ROOT)
     from molmodel_b200.water import water_box
     from oracle.oracle import reference, port, make_config
     lib = reference() or port()
     wb = water_box(NSIDE, seed=seed)
-    c = make_config(wb.box, **workload_cfg(wb.box))
+    wcfg = workload_cfg(wb.box)
+    c = make_config(wb.box, **wcfg)
     o = lib.eleclj(c, wb.nsite, wb.groups, wb.exclusions, wb.site_mask, wb.q, wb.sigma, wb.epsilon, wb.rscreen)
     for _ in range(n_warm):
         o.eval(wb.positions)
+    anchors = np.ascontiguousarray(wb.positions[0::3])
     conn.send(("ready", lib is reference()))
     conn.recv()
     times = []
@@ -371,15 +375,20 @@ def _ref_worker(conn, seed, n_warm, n_eval):
         o.eval(wb.positions)
         times.append(time.perf_counter() - t0)
     conn.send(("done", times))
+    nl = lib.nbrlist(wb.nwater, wcfg["rspace_cutoff"], wcfg["neighbor_list_width"], wb.box)
+    conn.recv()
+    t0 = time.perf_counter()
+    nl.update(anchors)  # a list that has never been built rebuilds (rebuild_periodic)
+    conn.send(("built", time.perf_counter() - t0))
 
 
 def cpu_baseline(wb, cfg, n_eval=3):
-    """The reference's own code (oracle/_ref) on 1 host core: 3 evaluations, the
-    first of which builds the neighbour list."""
+    """The reference's own code (oracle/_ref) on 1 host core: 3 evaluations
+    and one list build, the build amortised over 10 steps."""
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     a, b = ctx.Pipe()
-    pr = ctx.Process(target=_ref_worker, args=(b, wb.seed, 0, n_eval))
+    pr = ctx.Process(target=_ref_worker, args=(b, wb.seed, 1, n_eval))
     pr.start()
     try:
         os.sched_setaffinity(pr.pid, {sorted(os.sched_getaffinity(0))[0]})
@@ -388,32 +397,37 @@ def cpu_baseline(wb, cfg, n_eval=3):
     _, is_ref = a.recv()
     a.send("go")
     _, times = a.recv()
+    a.send("build")
+    _, build = a.recv()
     pr.join()
-    steady = min(times[1:]) if len(times) > 1 else times[0]
-    rebuild = max(times[0] - steady, 0.0)
-    per_step = steady + rebuild / 10
+    steady = min(times)
+    per_step = steady + build / 10
     return {"value": 1.0 / per_step, "unit": "steps/s", "cores": 1, "kind": "reference" if is_ref else "port",
-            "sample": f"{n_eval} evaluations of the same 98,304-site box on one pinned core, the list build "
-                      f"amortised over 10 steps: evaluation {steady:.2f} s, build {rebuild:.2f} s"}
+            "sample": f"{n_eval} evaluations of the same 98,304-site box on one pinned core (best taken) and "
+                      f"one list build amortised over 10 steps: evaluation {steady:.2f} s, build {build:.2f} s"}
 
 
 def run_reference(args):
-    """The reference's CPU code on every host core: independent processes,
-    each evaluating the workload; value = evaluations completed per second."""
+    """The reference's CPU code on every host core: P = min(cores, steps)
+    independent processes, each timing the same number of evaluations
+    m = ceil(steps / P) (so no process waits on a straggler's extra one), then
+    one list build each, all concurrently.  value = P / (t_eval + t_build / 10)
+    with t_eval the wall time of the evaluation phase / m and t_build that of
+    the build phase: the GPU arm's workload, whose list is rebuilt every 10
+    evaluations."""
     rank, world, local = dist_env()
     if rank != 0:
         return
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
-    total = max(1, args.steps)
-    per = [total // ncores + (1 if i < total % ncores else 0) for i in range(ncores)]
+    steps = max(1, args.steps)
+    nproc = min(ncores, steps)
+    m = -(-steps // nproc)
     procs, pipes = [], []
-    for i in range(ncores):
-        if per[i] == 0:
-            continue
+    for i in range(nproc):
         a, b = ctx.Pipe()
-        pr = ctx.Process(target=_ref_worker, args=(b, args.seed, 1 if args.warmup > 0 else 0, per[i]))
+        pr = ctx.Process(target=_ref_worker, args=(b, args.seed, 1 if args.warmup > 0 else 0, m))
         pr.start()
         procs.append(pr)
         pipes.append(a)
@@ -426,21 +440,31 @@ def run_reference(args):
         a.send("go")
     for a in pipes:
         a.recv()
-    wall = time.perf_counter() - t0
+    wall_eval = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for a in pipes:
+        a.send("build")
+    for a in pipes:
+        a.recv()
+    wall_build = time.perf_counter() - t0
     for pr in procs:
         pr.join()
-    value = total / wall
-    used = len(pipes)
-    out = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": total,
+    per_step = wall_eval / m + wall_build / 10
+    value = nproc / per_step
+    out = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": steps,
            "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded water lattice, random orientations",
            "config": {"workload": WORKLOAD, "precision": "fp64 (reference CPU code)",
-                      "parallelism": f"{used} independent processes, one evaluation at a time each",
-                      "list": "built once per process before timing (same coordinates every step)"},
+                      "parallelism": f"{nproc} independent processes, {m} timed evaluations each "
+                                     f"({nproc * m} in all), then one list build each",
+                      "list": "rebuilt every 10 evaluations: one timed reference list build per process, "
+                              "amortised over 10 steps",
+                      "phases_s": {"evaluations": wall_eval, "list_builds": wall_build}},
            "impl": "reference",
-           "cpu_baseline": {"value": value, "unit": "steps/s", "cores": used,
+           "cpu_baseline": {"value": value, "unit": "steps/s", "cores": nproc,
                             "kind": "reference" if is_ref else "port",
-                            "sample": f"{total} evaluations of the 98,304-site box over {used} processes"},
+                            "sample": f"{nproc * m} evaluations of the 98,304-site box over {nproc} processes "
+                                      f"({m} each) and {nproc} list builds"},
            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 

@@ -29,36 +29,90 @@ constexpr int kNoallocMaxDevices = 64;
 // [0, 3K) wave vectors, [3K, 4K) a_k, [4K, 6K) structure factor (cos, sin), [6K] count
 __device__ __align__(256) static double g_noalloc_kspace[6 * kNoallocMaxK + 8];
 
-// Wave vectors in the reference's order (src/kspace.c:35-58): the half space
-// of integer n with |n|^2 <= kc^2 + 1e-8, sorted by |n|^2, largest first,
-// ties kept in enumeration order.  One thread: the table has < 4096 entries.
-__global__ void k_noalloc_table(double kc, double rx, double ry, double rz, double volume, double eta,
-                                double *scratch)
+// Wave vectors in the order the k-sum walks them (src/kspace.c:35-58): the
+// half space of integer n with |n|^2 <= kc^2 + 1e-8, sorted by |n|^2, largest
+// first, ties in enumeration order (the reference's qsort does not promise a
+// tie order; ties only change the order of the floating-point sum).
+//
+// One warp ranks every point of the enumeration box (nx in [0, nmax], ny and
+// nz in [-nmax, nmax], lexicographic, i.e. the enumeration order) in two
+// passes over chunks of 32 consecutive points: the first counts the points of
+// each shell |n|^2 = s, lane 0 turns the counts into the first slot of each
+// shell (largest s first), and the second gives each point its slot = first
+// slot of its shell + points of the shell in earlier chunks + points of the
+// shell in earlier lanes of this chunk (__match_any_sync).  The box has at
+// most 14 x 27 x 27 = 10,206 points (kc <= 13.5), so each pass takes at most
+// 319 steps of the warp.
+constexpr int kNoallocMaxShell = 192;  // |n|^2 <= kc^2 + 1e-8 < 192 for kc <= kNoallocMaxCut
+constexpr double kNoallocMaxCut = 13.5;
+
+__global__ void __launch_bounds__(32) k_noalloc_table(double kc, double rx, double ry, double rz, double volume,
+                                                       double eta, double *scratch)
 {
-  if (blockIdx.x || threadIdx.x)
-    return;
+  __shared__ int first[kNoallocMaxShell + 1], seen[kNoallocMaxShell + 1];
+  const int lane = threadIdx.x;
   double *kvec = scratch, *ak = scratch + 3 * kNoallocMaxK;
   const double n2max = kc * kc + 1e-8;
   const int nmax = (int) floor(kc);
-  const int smax = (int) floor(n2max);
-  const double c = 0.25 / (eta * eta), f = 4 * M_PI / volume;
-  int nk = 0;
-  for (int s = smax; s >= 1; s--)
-    for (int nx = 0; nx <= nmax; nx++)
-      for (int ny = (nx == 0 ? 0 : -nmax); ny <= nmax; ny++)
-        for (int nz = (nx == 0 && ny == 0 ? 1 : -nmax); nz <= nmax; nz++) {
-          const int n2 = nx * nx + ny * ny + nz * nz;
-          if (n2 != s || nk >= kNoallocMaxK)
-            continue;
-          const double kx = rx * nx, ky = ry * ny, kz = rz * nz;
-          const double k2 = kx * kx + ky * ky + kz * kz;
-          kvec[3 * nk] = kx;
-          kvec[3 * nk + 1] = ky;
-          kvec[3 * nk + 2] = kz;
-          ak[nk] = f * exp(-k2 * c) / k2;
-          nk++;
-        }
-  scratch[6 * kNoallocMaxK] = nk;
+  const int side = 2 * nmax + 1;
+  const int nbox = (nmax + 1) * side * side;
+  for (int s = lane; s <= kNoallocMaxShell; s += 32) {
+    first[s] = 0;
+    seen[s] = 0;
+  }
+  __syncwarp();
+  // shell of enumeration point i, or -1 outside the half space or the cutoff
+  auto shell = [&](int i, int &nx, int &ny, int &nz) -> int {
+    if (i >= nbox)
+      return -1;
+    nx = i / (side * side);
+    ny = (i / side) % side - nmax;
+    nz = i % side - nmax;
+    if (nx == 0 && (ny < 0 || (ny == 0 && nz < 1)))
+      return -1;
+    const int n2 = nx * nx + ny * ny + nz * nz;
+    return n2 <= n2max ? n2 : -1;
+  };
+  for (int c = 0; c < nbox; c += 32) {
+    int nx, ny, nz;
+    const int s = shell(c + lane, nx, ny, nz);
+    if (s > 0)
+      atomicAdd(&first[s], 1);
+  }
+  __syncwarp();
+  if (lane == 0) {
+    int run = 0;
+    for (int s = kNoallocMaxShell; s >= 1; s--) {
+      const int n = first[s];
+      first[s] = run;
+      run += n;
+    }
+    scratch[6 * kNoallocMaxK] = run;
+  }
+  __syncwarp();
+  const double c2 = 0.25 / (eta * eta), f = 4 * M_PI / volume;
+  const unsigned lower = (1u << lane) - 1;
+  for (int c = 0; c < nbox; c += 32) {
+    int nx = 0, ny = 0, nz = 0;
+    const int s = shell(c + lane, nx, ny, nz);
+    const unsigned same = __match_any_sync(0xffffffffu, s);
+    if (s > 0) {
+      const int slot = first[s] + seen[s] + __popc(same & lower);
+      if (slot < kNoallocMaxK) {
+        const double kx = rx * nx, ky = ry * ny, kz = rz * nz;
+        const double k2 = kx * kx + ky * ky + kz * kz;
+        kvec[3 * slot] = kx;
+        kvec[3 * slot + 1] = ky;
+        kvec[3 * slot + 2] = kz;
+        ak[slot] = f * exp(-k2 * c2) / k2;
+      }
+    }
+    __syncwarp();
+    // the lowest lane of each shell present in this chunk advances its count
+    if (s > 0 && (same & lower) == 0)
+      seen[s] += __popc(same);
+    __syncwarp();
+  }
 }
 
 constexpr int kNoallocThreads = 256;
@@ -166,7 +220,16 @@ extern "C" int mmnb_kspace_field_noalloc(int nsite, const double *d_r, const dou
   }
   if (!(eta > 0) || !(kspace_cutoff > 0))
     return set_global_error(MMNB_ERR_ARG, "mmnb_kspace_field_noalloc: eta and kspace_cutoff must be > 0");
-  // count the wave vectors on the host to size the launches and check the limit
+  // Past a cutoff of 13.5 the half space holds more than the array's wave
+  // vectors whatever the box (a ball of radius 13.5 - sqrt(3)/2 alone gives
+  // 4219 half-space points), so such cutoffs, infinities and NaN are refused
+  // before any counting; below it the exact count is a loop of at most
+  // 14 x 27 x 27 steps.
+  if (!(kspace_cutoff <= kNoallocMaxCut))
+    return set_global_error(MMNB_ERR_ARG, "mmnb_kspace_field_noalloc: kspace_cutoff " +
+                                              std::to_string(kspace_cutoff) +
+                                              " needs more wave vectors than this entry point holds (at most " +
+                                              std::to_string(kNoallocMaxK) + ")");
   const double n2max = kspace_cutoff * kspace_cutoff + 1e-8;
   const int nmax = (int) floor(kspace_cutoff);
   long nk = 0;
@@ -191,7 +254,7 @@ extern "C" int mmnb_kspace_field_noalloc(int nsite, const double *d_r, const dou
   if (!scratch)
     return status;
   cudaStream_t s = (cudaStream_t) stream;
-  k_noalloc_table<<<1, 1, 0, s>>>(kspace_cutoff, 2 * M_PI * (1.0 / L[0]), 2 * M_PI * (1.0 / L[1]),
+  k_noalloc_table<<<1, 32, 0, s>>>(kspace_cutoff, 2 * M_PI * (1.0 / L[0]), 2 * M_PI * (1.0 / L[1]),
                                   2 * M_PI * (1.0 / L[2]), L[0] * L[1] * L[2], eta, scratch);
   k_noalloc_structure<<<(int) nk, kNoallocThreads, 0, s>>>(nsite, d_r, d_q, scratch);
   k_noalloc_field<<<div_up(nsite, 128), 128, 0, s>>>(nsite, (int) nk, d_r, scratch, d_phi, d_evec);
