@@ -390,7 +390,7 @@ void free_all(mmnb_handle *h)
                   h->d_phi, h->d_evec, h->d_ljf, h->d_lj_part, h->d_elec_part, h->d_energy, h->d_r, h->d_f,
                   h->d_mesh, h->d_meshk, h->d_green, h->d_kvec, h->d_egrid, h->d_egridk, h->d_mesh32,
                   h->d_meshk32, h->d_green32, h->d_mesh_fx, h->d_kint, h->d_kvecs, h->d_ak, h->d_skc,
-                  h->mx.site, h->mx.par, h->mx.anchor, h->mx.lj, h->mx.acc, h->mx.acck, h->d_wsum,
+                  h->mx.site, h->mx.par, h->mx.anchor, h->mx.acc, h->mx.acck, h->d_wsum,
                   h->d_bwd};
   for (void *p : ptrs)
     if (p)
@@ -681,7 +681,7 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
   CK(cudaMemset(h->d_wsum, 0, sizeof(unsigned long long) * 4));
   if (c->precision == MMNB_MIXED) {
     if ((s = dalloc(h, &h->mx.site, nslot)) || (s = dalloc(h, &h->mx.par, nslot)) ||
-        (s = dalloc(h, &h->mx.anchor, ngroup)) || (s = dalloc(h, &h->mx.lj, ngroup)) ||
+        (s = dalloc(h, &h->mx.anchor, ngroup)) ||
         (s = dalloc(h, &h->mx.acc, (size_t) nsite * kAccStride)) ||
         (s = dalloc(h, &h->mx.acck, (size_t) nsite * 4)))
       return s;

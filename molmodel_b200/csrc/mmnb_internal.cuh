@@ -57,10 +57,10 @@ struct Tuning {
 
 // Device buffers of the mixed-precision form.
 struct MixedBufs {
-  float4 *site = nullptr;        // sorted, padded slots: offset from the anchor (xyz), charge (w)
+  float4 *site = nullptr;        // sorted, padded slots: offset from the anchor (xyz), charge (w); or,
+                                 // for the rigid-water kernel, three packed slots per group
   float4 *par = nullptr;         // sorted, padded slots: sigma, sqrt(epsilon), rscreen, mask bits
   double4 *anchor = nullptr;     // sorted groups: anchor position (FP64)
-  float2 *lj = nullptr;          // sorted groups: anchor sigma, sqrt(epsilon)
   long long *acc = nullptr;      // per site (original order), kAccStride fixed-point values
   long long *acck = nullptr;     // per site (original order): P3M interpolation phi, Ex, Ey, Ez
 };

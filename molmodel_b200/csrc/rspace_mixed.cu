@@ -331,12 +331,25 @@ __global__ void __launch_bounds__(kMxWarps * 32) k_pair_mixed(MixedArgs a)
 // list 32 entries at a time: each lane tests one partner's FP64 anchor
 // distance (anchors are requested one batch ahead, list indices two batches
 // ahead), and for an accepted partner writes the FP32 anchor displacement to
-// a 64-slot shared-memory ring and starts asynchronous copies (cp.async) of
-// the partner's three site slots and LJ parameters into the same ring slot.
-// When 32 entries are queued every lane evaluates one group pair from shared
-// memory.  Per group pair the kernel forms the FORCE on each row site (q E,
-// plus LJ and switch terms on O) and the pair energies, and converts those 11
-// values to fixed point.
+// a 128-slot shared-memory ring and starts asynchronous copies (cp.async) of
+// the partner's 48-byte record into the same ring slot.  When 32 entries are
+// queued every lane evaluates one group pair from shared memory.  Per group
+// pair the kernel forms the FORCE on each row site (q E, plus LJ and switch
+// terms on O) and the pair energies, and converts those 11 values to fixed
+// point.
+//
+// The site-pair arithmetic runs two site pairs per instruction (sm_100's
+// packed FP32 add/mul/fma on register pairs): the nine site pairs of a group
+// pair are four packed pairs and one single one,
+//   O  x (H1, H2)          partner H sites against the row O,
+//   (H1, H2) x O           the row H sites against the partner O,
+//   (H1, H2) x (H1, H2)    each row H against the partner H of its own index,
+//   (H2, H1) x (H1, H2)    each row H against the other partner H,
+//   O  x O,
+// so the partner record is laid out in pairs: (h1x, h2x, h1y, h2y),
+// (h1z, h2z, q1, q2), (qO, qO, sigma, sqrt(epsilon)), with the H offsets
+// taken from the anchor O.  The multiply, add and fma of a packed pair round
+// each half exactly as the single instructions do.
 
 constexpr int kWaterRing = 128;
 // Warps (rows) per block of the rigid-water kernel: one, so a block retires as
@@ -350,8 +363,7 @@ struct WaterArgs {
   Box box;
   double rhi2;
   float rlo2, inv_sw, pe, c2, nel2;  // pe = p eta (erfc argument scale)
-  const float4 *site;     // 3 slots per sorted group: offset from anchor, charge
-  const float2 *lj;       // per sorted group: anchor sigma, sqrt(epsilon)
+  const float4 *site;     // 3 packed slots per sorted group (above)
   const double4 *anchor;
   const int *nbr, *nbr_count, *sorted, *group;
   long long *acc;         // per site: slots 4..6 receive the force, 0..3 are cleared
@@ -362,6 +374,62 @@ struct WaterArgs {
   double *plast;          // sorted anchors at the last prune
   int *flags;
   double rp2;
+};
+
+// a pair of FP32 values in one 64-bit register pair (the operand of the packed
+// f32x2 instructions)
+struct f2 {
+  unsigned long long v;
+};
+
+__device__ __forceinline__ f2 f2_pack(float lo, float hi)
+{
+  f2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ f2 f2_dup(float x) { return f2_pack(x, x); }
+__device__ __forceinline__ float f2_lo(f2 a)
+{
+  float lo;
+  asm("{\n .reg .f32 t;\n mov.b64 {%0, t}, %1;\n}" : "=f"(lo) : "l"(a.v));
+  return lo;
+}
+__device__ __forceinline__ float f2_hi(f2 a)
+{
+  float hi;
+  asm("{\n .reg .f32 t;\n mov.b64 {t, %0}, %1;\n}" : "=f"(hi) : "l"(a.v));
+  return hi;
+}
+__device__ __forceinline__ f2 add2(f2 a, f2 b)
+{
+  f2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b)
+{
+  f2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b)
+{
+  f2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c)
+{
+  f2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+  return r;
+}
+__device__ __forceinline__ f2 f2_of(unsigned long long v) { return f2{v}; }
+
+// erfc polynomial coefficients as packed constants
+struct ErfcConst2 {
+  f2 e[8];
 };
 
 // One site pair of a water group pair: adds q_j b1 S d to the row site's field
@@ -390,6 +458,36 @@ __device__ __forceinline__ void water_site(float dx, float dy, float dz, float q
   rinv_out = rinv;
 }
 
+// The same for two site pairs at once (the halves of each packed value are
+// independent site pairs): the arithmetic of water_site, half by half.
+struct WaterConst2 {
+  f2 pe, one, nel2, c2;
+};
+
+__device__ __forceinline__ void water_site2(f2 dx, f2 dy, f2 dz, f2 qb, f2 qbs, const WaterConst2 &c,
+                                            const ErfcConst2 &k, f2 &ex, f2 &ey, f2 &ez, f2 &tq)
+{
+  const f2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+  const f2 rinv = f2_pack(rsqrt_approx(f2_lo(r2)), rsqrt_approx(f2_hi(r2)));
+  const f2 targ = fma2(c.pe, mul2(r2, rinv), c.one);
+  const f2 t = f2_pack(rcp_approx(f2_lo(targ)), rcp_approx(f2_hi(targ)));
+  f2 p = fma2(k.e[7], t, k.e[6]);
+  p = fma2(p, t, k.e[5]);
+  p = fma2(p, t, k.e[4]);
+  p = fma2(p, t, k.e[3]);
+  p = fma2(p, t, k.e[2]);
+  p = fma2(p, t, k.e[1]);
+  p = fma2(p, t, k.e[0]);
+  const f2 earg = mul2(r2, c.nel2);
+  const f2 e = f2_pack(ex2_approx(f2_lo(earg)), ex2_approx(f2_hi(earg)));
+  const f2 b0 = mul2(mul2(t, p), mul2(e, rinv));
+  tq = fma2(qb, b0, tq);
+  const f2 f = mul2(mul2(fma2(c.c2, e, b0), mul2(rinv, rinv)), qbs);
+  ex = fma2(f, dx, ex);
+  ey = fma2(f, dy, ey);
+  ez = fma2(f, dz, ez);
+}
+
 // Minimum-image anchor displacement with contracted FP64 arithmetic (fewer
 // instructions than the reference-rounded form the FP64 kernels use).  The
 // decision it feeds only matters at r = rc, where the switch and its
@@ -414,13 +512,6 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src)
                : "memory");
 }
 
-__device__ __forceinline__ void cp_async8(void *dst, const void *src)
-{
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned) __cvta_generic_to_shared(dst)),
-               "l"(src)
-               : "memory");
-}
-
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
@@ -430,10 +521,9 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 template <int MINB>
 __global__ void __launch_bounds__(kWaterWarps * 32, MINB * kMxWarps / kWaterWarps) k_pair_water(WaterArgs a)
 {
-  // per warp: ring of anchor displacement (xyz, r^2), partner O slot (zero
-  // offset, charge), H1 and H2 slots (offset, charge); LJ parameters apart
+  // per warp: ring of anchor displacement (xyz, r^2) and the partner's three
+  // packed slots
   __shared__ float4 ring[kWaterWarps][4][kWaterRing];
-  __shared__ float2 ql[kWaterWarps][kWaterRing];   // partner sigma, sqrt(eps)
   constexpr int kCols = 11;
   constexpr int kMask = kWaterRing - 1;
   constexpr float kTwo32 = 4294967296.0f, kTwo31 = 2147483648.0f;
@@ -446,14 +536,30 @@ __global__ void __launch_bounds__(kWaterWarps * 32, MINB * kMxWarps / kWaterWarp
   float4 *qa = ring[w][0], *q0 = ring[w][1], *q1 = ring[w][2], *q2 = ring[w][3];
   int si0 = 0;
   if (p < a.ngroup) {
-    const float qO = a.site[3 * (size_t) p].w;
-    const float4 h1 = a.site[3 * (size_t) p + 1];
-    const float4 h2 = a.site[3 * (size_t) p + 2];
-    const float2 ljo = a.lj[p];
+    // the row's own record: H offsets and charges, O charge and LJ parameters
+    const float4 r0 = a.site[3 * (size_t) p], r1 = a.site[3 * (size_t) p + 1], r2 = a.site[3 * (size_t) p + 2];
     const double4 ai = a.anchor[p];
+    const f2 h12x = f2_pack(r0.x, r0.y), h12y = f2_pack(r0.z, r0.w), h12z = f2_pack(r1.x, r1.y);
+    const f2 h21x = f2_pack(r0.y, r0.x), h21y = f2_pack(r0.w, r0.z), h21z = f2_pack(r1.y, r1.x);
+    const float qO = r2.x, qH1 = r1.z, qH2 = r1.w;
+    const float2 ljo = make_float2(r2.z, r2.w);
     // charges times the fixed-point scale: the converted values come out of
     // the last product directly
-    const float qO32 = qO * kTwo32, qH1_32 = h1.w * kTwo32, qH2_32 = h2.w * kTwo32;
+    const float qO32 = qO * kTwo32, qH1_32 = qH1 * kTwo32, qH2_32 = qH2 * kTwo32;
+    WaterConst2 c2;
+    c2.pe = f2_dup(a.pe);
+    c2.one = f2_dup(1.f);
+    c2.nel2 = f2_dup(a.nel2);
+    c2.c2 = f2_dup(a.c2);
+    ErfcConst2 ke;
+    ke.e[0] = f2_dup(kE0);
+    ke.e[1] = f2_dup(kE1);
+    ke.e[2] = f2_dup(kE2);
+    ke.e[3] = f2_dup(kE3);
+    ke.e[4] = f2_dup(kE4);
+    ke.e[5] = f2_dup(kE5);
+    ke.e[6] = f2_dup(kE6);
+    ke.e[7] = f2_dup(kE7);
     si0 = a.group[2 * a.sorted[p]];
     // full rows (and make the pruned ones), or the pruned rows
     const bool make = a.pnbr && a.flags[kFlagPruneFull];
@@ -464,38 +570,49 @@ __global__ void __launch_bounds__(kWaterWarps * 32, MINB * kMxWarps / kWaterWarp
     int pn = 0;
     const unsigned below = (1u << lane) - 1;
     auto compute = [&](int k) {
-      const float4 da = qa[k], j1 = q1[k], j2 = q2[k];
-      const float qj = q0[k].w;
-      const float2 lj = ql[w][k];
-      const float r2a = da.w;
-      float s = 1.f, ds = 0.f;
-      if (r2a > a.rlo2) {
-        const float z = (r2a - a.rlo2) * a.inv_sw;
-        s = fmaf(fmaf(fmaf(-6.f, z, 15.f), z, -10.f), z * z * z, 1.f);
-        ds = fmaf(fmaf(60.f, z, -120.f), z, 60.f) * z * z * a.inv_sw;
-      }
-      const float qbO = qj * s, qb1 = j1.w * s, qb2 = j2.w * s;
-      float eOx = 0.f, eOy = 0.f, eOz = 0.f, e1x = 0.f, e1y = 0.f, e1z = 0.f, e2x = 0.f, e2y = 0.f, e2z = 0.f;
-      float tO = 0.f, t1 = 0.f, t2 = 0.f, rOO, rtmp;
-      // row O (offset 0)
-      water_site(da.x, da.y, da.z, qj, qbO, a, eOx, eOy, eOz, tO, rOO);
-      water_site(da.x - j1.x, da.y - j1.y, da.z - j1.z, j1.w, qb1, a, eOx, eOy, eOz, tO, rtmp);
-      water_site(da.x - j2.x, da.y - j2.y, da.z - j2.z, j2.w, qb2, a, eOx, eOy, eOz, tO, rtmp);
-      // row H1
-      const float c1x = da.x + h1.x, c1y = da.y + h1.y, c1z = da.z + h1.z;
-      water_site(c1x, c1y, c1z, qj, qbO, a, e1x, e1y, e1z, t1, rtmp);
-      water_site(c1x - j1.x, c1y - j1.y, c1z - j1.z, j1.w, qb1, a, e1x, e1y, e1z, t1, rtmp);
-      water_site(c1x - j2.x, c1y - j2.y, c1z - j2.z, j2.w, qb2, a, e1x, e1y, e1z, t1, rtmp);
-      // row H2
-      const float c2x = da.x + h2.x, c2y = da.y + h2.y, c2z = da.z + h2.z;
-      water_site(c2x, c2y, c2z, qj, qbO, a, e2x, e2y, e2z, t2, rtmp);
-      water_site(c2x - j1.x, c2y - j1.y, c2z - j1.z, j1.w, qb1, a, e2x, e2y, e2z, t2, rtmp);
-      water_site(c2x - j2.x, c2y - j2.y, c2z - j2.z, j2.w, qb2, a, e2x, e2y, e2z, t2, rtmp);
+      const float4 da = qa[k];
+      const ulonglong2 j0 = *reinterpret_cast<const ulonglong2 *>(&q0[k]);
+      const ulonglong2 j1 = *reinterpret_cast<const ulonglong2 *>(&q1[k]);
+      const float4 j2 = q2[k];
+      const f2 jx = f2_of(j0.x), jy = f2_of(j0.y), jz = f2_of(j1.x), qj = f2_of(j1.y);
+      const float qjO = j2.x;
+      // switch S(z) and dS/dr^2 (zero inside rc - width), branch-free
+      const float z = fmaxf(da.w - a.rlo2, 0.f) * a.inv_sw;
+      const float zz = z * z;
+      const float s = fmaf(fmaf(fmaf(-6.f, z, 15.f), z, -10.f), zz * z, 1.f);
+      const float ds = fmaf(fmaf(60.f, z, -120.f), z, 60.f) * zz * a.inv_sw;
+      const f2 s2 = f2_dup(s);
+      const f2 qbs = mul2(qj, s2);
+      const f2 q0d = f2_pack(j2.x, j2.y);
+      const f2 q0s = mul2(q0d, s2);
+      const f2 dx = f2_dup(da.x), dy = f2_dup(da.y), dz = f2_dup(da.z);
+      // row O against partner O (single) and partner H1, H2 (packed)
+      float eOx = 0.f, eOy = 0.f, eOz = 0.f, tO = 0.f, rOO;
+      water_site(da.x, da.y, da.z, qjO, qjO * s, a, eOx, eOy, eOz, tO, rOO);
+      f2 aOx = f2_dup(0.f), aOy = aOx, aOz = aOx, aOt = aOx;
+      water_site2(sub2(dx, jx), sub2(dy, jy), sub2(dz, jz), qj, qbs, c2, ke, aOx, aOy, aOz, aOt);
+      // rows H1, H2 against partner O, then against partner H1, H2 in order
+      const f2 cx = add2(dx, h12x), cy = add2(dy, h12y), cz = add2(dz, h12z);
+      f2 hx = f2_dup(0.f), hy = hx, hz = hx, ht = hx;
+      water_site2(cx, cy, cz, q0d, q0s, c2, ke, hx, hy, hz, ht);
+      water_site2(sub2(cx, jx), sub2(cy, jy), sub2(cz, jz), qj, qbs, c2, ke, hx, hy, hz, ht);
+      // rows H2, H1 against partner H1, H2
+      f2 wx = f2_dup(0.f), wy = wx, wz = wx, wt = wx;
+      water_site2(sub2(add2(dx, h21x), jx), sub2(add2(dy, h21y), jy), sub2(add2(dz, h21z), jz), qj, qbs, c2, ke,
+                  wx, wy, wz, wt);
+      eOx += f2_lo(aOx) + f2_hi(aOx);
+      eOy += f2_lo(aOy) + f2_hi(aOy);
+      eOz += f2_lo(aOz) + f2_hi(aOz);
+      tO += f2_lo(aOt) + f2_hi(aOt);
+      const float e1x = f2_lo(hx) + f2_hi(wx), e1y = f2_lo(hy) + f2_hi(wy), e1z = f2_lo(hz) + f2_hi(wz);
+      const float e2x = f2_hi(hx) + f2_lo(wx), e2y = f2_hi(hy) + f2_lo(wy), e2z = f2_hi(hz) + f2_lo(wz);
+      const float t1 = f2_lo(ht) + f2_hi(wt), t2 = f2_hi(ht) + f2_lo(wt);
       // O-O Lennard-Jones
-      const float sg = a.geometric ? ljo.x * lj.x : 0.5f * (ljo.x + lj.x);
-      const float s2 = a.geometric ? sg : sg * sg;
-      const float s6 = s2 * s2 * s2;
-      const float b = 4.f * ljo.y * lj.y * s6;
+      const float sj = j2.z, ej = j2.w;
+      const float sg = a.geometric ? ljo.x * sj : 0.5f * (ljo.x + sj);
+      const float sq = a.geometric ? sg : sg * sg;
+      const float s6 = sq * sq * sq;
+      const float b = 4.f * ljo.y * ej * s6;
       const float ir2 = rOO * rOO;
       const float ir6 = ir2 * ir2 * ir2;
       const float bi6 = b * ir6;
@@ -504,7 +621,7 @@ __global__ void __launch_bounds__(kWaterWarps * 32, MINB * kMxWarps / kWaterWarp
       const float du = (12.f * ai12 - 6.f * bi6) * ir2 * s;
       // unswitched Coulomb energy of the group pair; its switched half is the
       // row's energy share and, with u, it scales the switch derivative
-      const float tq = fmaf(qO, tO, fmaf(h1.w, t1, h2.w * t2));
+      const float tq = fmaf(qO, tO, fmaf(qH1, t1, qH2 * t2));
       const float g = ds * (tq + u);
       const float fo32 = (du + g) * kTwo32;
       const float s31 = s * kTwo31;
@@ -548,7 +665,6 @@ __global__ void __launch_bounds__(kWaterWarps * 32, MINB * kMxWarps / kWaterWarp
         cp_async16(&q0[slot], src);
         cp_async16(&q1[slot], src + 1);
         cp_async16(&q2[slot], src + 2);
-        cp_async8(&ql[w][slot], a.lj + jc);
       }
       cp_async_commit();
       // entries of earlier batches are evaluated one batch after their copies
@@ -632,7 +748,6 @@ cudaError_t launch_rspace_water(mmnb_handle *h)
   a.c2 = (float) (h->eta * M_2_SQRTPI);
   a.nel2 = (float) (-h->eta * h->eta * M_LOG2E);
   a.site = h->mx.site;
-  a.lj = h->mx.lj;
   a.anchor = h->mx.anchor;
   a.nbr = h->d_nbr;
   a.nbr_count = h->d_nbr_count;
@@ -654,46 +769,61 @@ cudaError_t launch_rspace_water(mmnb_handle *h)
   return cudaGetLastError();
 }
 
-// Per step: sorted, padded FP32 slots (offset from anchor, charge, LJ
-// parameters, mask) and the FP64 anchors.
+// Per step: sorted FP32 slots and the FP64 anchors.  General layout (any
+// groups, k_pair_mixed): per group G slots of (offset from anchor, charge) and
+// (sigma, sqrt(epsilon), rscreen, mask), padded with empty slots.  Rigid-water
+// layout (k_pair_water): per group three packed slots, (h1x, h2x, h1y, h2y),
+// (h1z, h2z, q1, q2), (qO, qO, sigma_O, sqrt(epsilon_O)).
 __global__ void k_prep_mixed(const double *__restrict__ r, const double *__restrict__ q,
                              const double *__restrict__ sig, const double *__restrict__ eps,
                              const double *__restrict__ rscreen, const int *__restrict__ mask,
                              const int *__restrict__ sorted, const int *__restrict__ group, int ngroup, int G,
-                             float4 *__restrict__ site, float4 *__restrict__ par, double4 *__restrict__ anchor,
-                             float2 *__restrict__ lj, unsigned long long *__restrict__ wsum)
+                             int water, float4 *__restrict__ site, float4 *__restrict__ par,
+                             double4 *__restrict__ anchor, unsigned long long *__restrict__ wsum)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < 2)
     wsum[s] = 0ull;
-  if (s < ngroup * G) {
-    const int p = s / G, k = s % G;
-    const int g = sorted[p];
-    const int a0 = group[2 * g];
-    const int st = a0 + k;
-    const double ax = r[3 * a0], ay = r[3 * a0 + 1], az = r[3 * a0 + 2];
-    if (k == 0) {
-      anchor[p] = make_double4(ax, ay, az, 0.0);
-      lj[p] = make_float2((float) sig[a0], (float) sqrt(eps[a0]));
-    }
-    if (st < group[2 * g + 1]) {
-      const float ox = (float) (r[3 * st] - ax), oy = (float) (r[3 * st + 1] - ay),
-                  oz = (float) (r[3 * st + 2] - az);
-      site[s] = make_float4(ox, oy, oz, (float) q[st]);
-      par[s] = make_float4((float) sig[st], (float) sqrt(eps[st]), (float) rscreen[st], __int_as_float(mask[st]));
-    } else {
-      site[s] = make_float4(0.f, 0.f, 0.f, 0.f);
-      par[s] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
-    }
+  if (s >= ngroup * G)
+    return;
+  const int p = s / G, k = s % G;
+  const int g = sorted[p];
+  const int a0 = group[2 * g];
+  const double ax = r[3 * a0], ay = r[3 * a0 + 1], az = r[3 * a0 + 2];
+  if (k == 0)
+    anchor[p] = make_double4(ax, ay, az, 0.0);
+  if (water) {
+    // G == 3: slot k of group p from the two H sites (a0 + 1, a0 + 2) and O
+    const int h1 = a0 + 1, h2 = a0 + 2;
+    float4 v;
+    if (k == 0)
+      v = make_float4((float) (r[3 * h1] - ax), (float) (r[3 * h2] - ax), (float) (r[3 * h1 + 1] - ay),
+                      (float) (r[3 * h2 + 1] - ay));
+    else if (k == 1)
+      v = make_float4((float) (r[3 * h1 + 2] - az), (float) (r[3 * h2 + 2] - az), (float) q[h1], (float) q[h2]);
+    else
+      v = make_float4((float) q[a0], (float) q[a0], (float) sig[a0], (float) sqrt(eps[a0]));
+    site[s] = v;
+    return;
+  }
+  const int st = a0 + k;
+  if (st < group[2 * g + 1]) {
+    const float ox = (float) (r[3 * st] - ax), oy = (float) (r[3 * st + 1] - ay), oz = (float) (r[3 * st + 2] - az);
+    site[s] = make_float4(ox, oy, oz, (float) q[st]);
+    par[s] = make_float4((float) sig[st], (float) sqrt(eps[st]), (float) rscreen[st], __int_as_float(mask[st]));
+  } else {
+    site[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+    par[s] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
   }
 }
 
 cudaError_t launch_prep_mixed(mmnb_handle *h, const double *d_r)
 {
   const int n = h->ngroup * h->G;
+  const int water = h->water && !h->want_fields && h->cfg.include_rspace;
   k_prep_mixed<<<div_up(n, 256), 256, 0, h->stream>>>(d_r, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_mask,
-                                                      h->d_sorted, h->d_group, h->ngroup, h->G, h->mx.site,
-                                                      h->mx.par, h->mx.anchor, h->mx.lj, h->d_wsum);
+                                                      h->d_sorted, h->d_group, h->ngroup, h->G, water, h->mx.site,
+                                                      h->mx.par, h->mx.anchor, h->d_wsum);
   h->launches += 1;
   return cudaGetLastError();
 }
