@@ -47,9 +47,37 @@ double sq(double x) { return x * x; }
 // 64 machine epsilons, the reference's is_almost_zero (src/fns.c:8-31)
 bool almost_zero(double x) { return fabs(x) < 64 * 2.220446049250313e-16; }
 
-// The reference's Chebyshev table, same formula and operation order
-// (src/cheby.c:7-45, src/rspace.c:18-37); built on the host so it is bitwise
-// the table RSpaceChebyshev_new builds.
+// Segment i of the reference's Chebyshev table, same formula and operation
+// order (src/cheby.c:7-45, src/rspace.c:18-37): built on the host so segments
+// 0..511 are bitwise the ones RSpaceChebyshev_new builds.  Segments past 511
+// continue the same construction beyond the reference's range (the rigid-water
+// FP64 kernel reads them for site pairs beyond 1.2 rc^2).
+void chebyshev_segment(int i, double r2min, double dx, double eta, double *o)
+{
+  const double a = i * dx + r2min, b = (i + 1) * dx + r2min;
+  double g[50], c[4];
+  const double fac = 2.0 / 50;
+  const double bma = 0.5 * (b - a), bpa = 0.5 * (b + a);
+  for (int k = 0; k < 50; k++) {
+    const double r2 = cos(M_PI * (k + 0.5) / 50) * bma + bpa;
+    const double r = sqrt(r2);
+    g[k] = erfc(eta * r) / r;
+  }
+  for (int j = 0; j < 4; j++) {
+    double s = 0;
+    for (int k = 0; k < 50; k++)
+      s += g[k] * cos(M_PI * j * (k + 0.5) / 50);
+    c[j] = fac * s;
+  }
+  o[0] = c[0] / 2 - c[1] + c[2] - c[3];
+  o[1] = 2 * c[1] - 8 * c[2] + 18 * c[3];
+  o[2] = 8 * c[2] - 48 * c[3];
+  o[3] = 32 * c[3];
+  o[4] = -2 * o[1] / (b - a);
+  o[5] = -2 * 2 * o[2] / (b - a);
+  o[6] = -2 * 3 * o[3] / (b - a);
+}
+
 void chebyshev_table(double rhi, double eta, double *mn, double *mx, double *inv_dx, double *coeff7)
 {
   const double r2max = 1.2 * sq(rhi);
@@ -58,31 +86,8 @@ void chebyshev_table(double rhi, double eta, double *mn, double *mx, double *inv
   *mn = r2min;
   *mx = r2max;
   *inv_dx = 1.0 / dx;
-  for (int i = 0; i < kCheb; i++) {
-    const double a = i * dx + r2min, b = (i + 1) * dx + r2min;
-    double g[50], c[4];
-    const double fac = 2.0 / 50;
-    const double bma = 0.5 * (b - a), bpa = 0.5 * (b + a);
-    for (int k = 0; k < 50; k++) {
-      const double r2 = cos(M_PI * (k + 0.5) / 50) * bma + bpa;
-      const double r = sqrt(r2);
-      g[k] = erfc(eta * r) / r;
-    }
-    for (int j = 0; j < 4; j++) {
-      double s = 0;
-      for (int k = 0; k < 50; k++)
-        s += g[k] * cos(M_PI * j * (k + 0.5) / 50);
-      c[j] = fac * s;
-    }
-    double *o = coeff7 + 7 * i;
-    o[0] = c[0] / 2 - c[1] + c[2] - c[3];
-    o[1] = 2 * c[1] - 8 * c[2] + 18 * c[3];
-    o[2] = 8 * c[2] - 48 * c[3];
-    o[3] = 32 * c[3];
-    o[4] = -2 * o[1] / (b - a);
-    o[5] = -2 * 2 * o[2] / (b - a);
-    o[6] = -2 * 3 * o[3] / (b - a);
-  }
+  for (int i = 0; i < kCheb; i++)
+    chebyshev_segment(i, r2min, dx, eta, coeff7 + 7 * i);
 }
 
 // nearest 2^a 3^b 5^c 7^d; ties keep the first found (src/pppm.c:277-292)
@@ -278,7 +283,29 @@ int setup_cheb(mmnb_handle *h)
   for (int i = 0; i < kCheb; i++)
     for (int k = 0; k < 7; k++)
       c8[8 * i + k] = c7[7 * i + k];
-  return upload(h, &h->d_cheb, c8);
+  int s = upload(h, &h->d_cheb, c8);
+  if (s)
+    return s;
+  // the rigid-water FP64 kernel's copy: the cubic's coefficients only, as two
+  // arrays of (c0, c1) and (c2, c3), continued to (rc + 2.5)^2 so every site
+  // pair of a water group pair within rc falls inside it
+  const double dx = (h->cheb_max - h->cheb_min) / kCheb;
+  const double r2ext = sq(h->rc + 2.5);
+  h->cheb_w_nseg = std::max(kCheb, std::min(kChebWMax, (int) ceil((r2ext - h->cheb_min) * h->cheb_inv_dx)));
+  std::vector<double> w(4 * (size_t) h->cheb_w_nseg);
+  for (int i = 0; i < h->cheb_w_nseg; i++) {
+    double o[7];
+    if (i < kCheb)
+      std::copy(c7.begin() + 7 * i, c7.begin() + 7 * i + 7, o);
+    else
+      chebyshev_segment(i, h->cheb_min, dx, h->eta, o);
+    w[2 * i] = o[0];
+    w[2 * i + 1] = o[1];
+    w[2 * ((size_t) h->cheb_w_nseg + i)] = o[2];
+    w[2 * ((size_t) h->cheb_w_nseg + i) + 1] = o[3];
+  }
+  h->water64_grid = 0;  // the kernel's shared-memory size follows the table
+  return upload(h, &h->d_cheb_w, w);
 }
 
 // reciprocal lattice 2 pi inv(latv)^T of the diagonal box
@@ -382,7 +409,7 @@ void free_all(mmnb_handle *h)
     h->ev_flags = nullptr;
   }
   void *ptrs[] = {h->d_group, h->d_excl_ptr, h->d_excl_idx, h->d_p14_ptr, h->d_p14_idx, h->d_gexcl_ptr,
-                  h->d_gexcl_idx, h->d_mask, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_cheb,
+                  h->d_gexcl_idx, h->d_mask, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_cheb, h->d_cheb_w, h->d_lj_row,
                   h->d_stencil, h->d_cell_rank, h->d_cell_of_rank, h->d_cell_of_group, h->d_cell_count,
                   h->d_cell_start, h->d_slot, h->d_sorted, h->d_rank, h->d_anchor, h->d_last, h->d_anchor_sorted, h->d_anchor32, h->d_block_sum,
                   h->d_top2, h->d_nbr, h->d_nbr_count, h->d_pnbr, h->d_pcount, h->d_plast, h->d_flags, h->d_sr,
@@ -673,6 +700,7 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
   const size_t nlj = (size_t) h->lj_pair_blocks + h->lj_excl_blocks;
   if ((s = dalloc(h, &h->d_phi, nsite)) || (s = dalloc(h, &h->d_evec, 3 * (size_t) nsite)) ||
       (s = dalloc(h, &h->d_ljf, 3 * (size_t) nsite)) || (s = dalloc(h, &h->d_lj_part, nlj)) ||
+      (s = dalloc(h, &h->d_lj_row, ngroup)) ||
       (s = dalloc(h, &h->d_elec_part, h->elec_blocks)) || (s = dalloc(h, &h->d_energy, 8)) ||
       (s = dalloc(h, &h->d_r, 3 * (size_t) nsite)) || (s = dalloc(h, &h->d_f, 3 * (size_t) nsite)) ||
       (s = dalloc(h, &h->d_wsum, 4)))
@@ -877,18 +905,26 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
   // corrections) assigns them, so they need clearing only without real space
   if (!h->cfg.include_rspace)
     CK(zero_site_arrays());
+  // FP64 rigid water: its own kernel (any request, site fields included)
+  const bool water64 = !mixed && h->water && h->cfg.include_rspace;
   if (mixed)
     CK(launch_prep_mixed(h, d_r));
+  else if (water64)
+    CK(launch_sort_water64(h, d_r));
   else
     CK(launch_sort_sites(h, d_r));
   timing_mark(h, "sort_sites");
   h->used_water = false;
+  h->used_water64 = false;
   if (h->cfg.include_rspace) {
     if (mixed && h->water && !h->want_fields) {
       CK(launch_rspace_water(h));
       h->used_water = true;
     } else if (mixed) {
       CK(launch_rspace_mixed(h));
+    } else if (water64) {
+      CK(launch_rspace_water64(h));
+      h->used_water64 = true;
     } else {
       CK(launch_rspace_fp64(h));
     }

@@ -24,6 +24,8 @@ struct FinArgs {
   // energy reduction
   const double *lj_part;              // per-block LJ partials [lj_lo, lj_hi)
   int lj_lo, lj_hi, any_q;
+  const double *lj_row;               // FP64 water kernel: per-row LJ energies [0, nrow), or null
+  int nrow;
   const unsigned long long *wsum;     // water kernel's fixed-point pair energies, or null
   unsigned long long *counter;        // finished-block counter, left at 0
   double tail;
@@ -111,6 +113,9 @@ __global__ void __launch_bounds__(kFinThreads) k_finalize(FinArgs a)
     el += a.elec_part[k];
   for (int k = a.lj_lo + threadIdx.x; k < a.lj_hi; k += blockDim.x)
     lj += a.lj_part[k];
+  if (a.lj_row)
+    for (int k = threadIdx.x; k < a.nrow; k += blockDim.x)
+      lj += a.lj_row[k];
   el = block_sum(el, se);
   lj = block_sum(lj, se);
   if (threadIdx.x == 0) {
@@ -149,7 +154,9 @@ cudaError_t launch_finalize(mmnb_handle *h, double *d_f, double *d_energy)
   a.lj_part = h->d_lj_part;
   // the water kernel leaves its LJ energy in the fixed-point word, not in the
   // pair partials
-  a.lj_lo = h->used_water ? h->lj_pair_blocks : 0;
+  a.lj_lo = (h->used_water || h->used_water64) ? h->lj_pair_blocks : 0;
+  a.lj_row = h->used_water64 ? h->d_lj_row : nullptr;
+  a.nrow = h->ngroup;
   a.lj_hi = h->lj_pair_blocks + h->lj_excl_blocks;
   a.any_q = h->any_q ? 1 : 0;
   a.wsum = h->used_water ? h->d_wsum : nullptr;

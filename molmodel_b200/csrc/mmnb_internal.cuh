@@ -12,6 +12,7 @@
 namespace mmnb {
 
 constexpr int kCheb = 512;          // Chebyshev segments (include/cheby.h:10)
+constexpr int kChebWMax = 2048;     // segments of the rigid-water FP64 kernel's continued table
 constexpr int kMaxGroup = 8;        // sites per group handled by the pair kernels
 constexpr int kMaxOrder = 7;        // P3M assignment order (src/pppm.c:61)
 constexpr int kWarp = 32;
@@ -99,6 +100,7 @@ struct mmnb_handle {
   bool water = false;                // every group is [O(q, LJ), H(q), H(q)] with no screening or group exclusions
   bool want_fields = false;          // this evaluation must produce per-site potential and field
   bool used_water = false;           // the last evaluation ran the water kernel
+  bool used_water64 = false;         // the last evaluation ran the FP64 water kernel
   double totA = 0, totB = 0, lj_correction = 0, neutral_b = 0;
 
   // host topology
@@ -117,6 +119,11 @@ struct mmnb_handle {
   double *d_q = nullptr, *d_sig = nullptr, *d_eps = nullptr, *d_rscreen = nullptr;
   double *d_cheb = nullptr;          // 512 x 8 doubles (7 used) + nothing else
   double cheb_min = 0, cheb_max = 0, cheb_inv_dx = 0;
+  // the rigid-water FP64 kernel's table: cheb_w_nseg x (c0, c1), then x (c2, c3)
+  double *d_cheb_w = nullptr;
+  int cheb_w_nseg = 0;
+  int water64_grid = 0;              // persistent blocks of that kernel (0: not sized yet)
+  size_t water64_smem = 0;
 
   // neighbour list
   mmnb::CellGeom cg{};
@@ -164,6 +171,7 @@ struct mmnb_handle {
   // outputs (original order)
   double *d_phi = nullptr, *d_evec = nullptr, *d_ljf = nullptr;
   double *d_lj_part = nullptr;       // LJ energy partials: pair-kernel blocks, then exclusion blocks
+  double *d_lj_row = nullptr;        // FP64 water kernel: LJ energy of each row (sorted order)
   // [0], [1]: fixed-point Coulomb and LJ pair energies of the water kernel;
   // [2]: block counter of the finalize kernel's last-block reduction
   unsigned long long *d_wsum = nullptr;
@@ -239,6 +247,8 @@ cudaError_t launch_rspace_fp64(mmnb_handle *h);
 cudaError_t launch_prep_mixed(mmnb_handle *h, const double *d_r);
 cudaError_t launch_rspace_mixed(mmnb_handle *h);
 cudaError_t launch_rspace_water(mmnb_handle *h);
+cudaError_t launch_sort_water64(mmnb_handle *h, const double *d_r);
+cudaError_t launch_rspace_water64(mmnb_handle *h);
 cudaError_t launch_exclusions(mmnb_handle *h, const double *d_r);
 cudaError_t launch_p3m_green(mmnb_handle *h);
 // stage bit 1: spread + FFT round trip, bit 2: gather
