@@ -266,6 +266,23 @@ int mmnb_set_tuning(mmnb_handle *h, const int tuning[3]);
 int mmnb_backward(mmnb_handle *h, const double *r, const double *dl_df, double *f, double *u,
                   double grad_u[3], double grad_l[3]);
 
+/* ---- virial ----------------------------------------------------------------
+   One evaluation at r (forces ADDED to f, energy ADDED to u, breakdown in e;
+   each may be NULL) and w = dU/ds at s = 1 along the path of the reference's
+   volume moves: MSys::scale (src/msys.cpp:416-421) translates every molecule
+   rigidly so its centre of mass is multiplied by s and scales the box, and
+   ElecLJ::scale (src/eleclj.cpp:1268-1280) divides eta and, through p3m_scale
+   (src/pppm.c:643-664), the influence function by s, keeping rc, the switch and
+   the mesh counts -- the path mmnb_scale follows.  The reference has no virial;
+   MSimProgram::test_scale (src/msimprog.cpp:379-400) evaluates the energy on
+   both sides of one such step.  dU/dV = w / (3 V), so the molecular pressure is
+   P = (N_mol k T - w / 3) / V.
+   Molecules: nmol half-open site ranges mol[2m], mol[2m+1] covering every site
+   once; site_mass (nsite): the masses that define their centres.  FP64 sums on
+   the GPU in a fixed order.  MMNB_ERR_UNSUPPORTED for screened charges. */
+int mmnb_virial(mmnb_handle *h, const double *r, int nmol, const int *mol, const double *site_mass, double *f,
+                double *u, mmnb_energy *e, double *w);
+
 /* ---- potential at points ---------------------------------------------------
    Electrostatic potential of the sites at r (3*nsite, host) at npoint points
    (3*npoint, host), written to phi[npoint] in the units of mmnb_compute's phi

@@ -47,22 +47,18 @@ double sq(double x) { return x * x; }
 // 64 machine epsilons, the reference's is_almost_zero (src/fns.c:8-31)
 bool almost_zero(double x) { return fabs(x) < 64 * 2.220446049250313e-16; }
 
-// Segment i of the reference's Chebyshev table, same formula and operation
-// order (src/cheby.c:7-45, src/rspace.c:18-37): built on the host so segments
-// 0..511 are bitwise the ones RSpaceChebyshev_new builds.  Segments past 511
-// continue the same construction beyond the reference's range (the rigid-water
-// FP64 kernel reads them for site pairs beyond 1.2 rc^2).
-void chebyshev_segment(int i, double r2min, double dx, double eta, double *o)
+// Cubic Chebyshev fit of g(r^2) on segment i, the reference's construction
+// (src/cheby.c:7-45: 50 nodes, coefficients turned into a power series in the
+// position inside the segment), then the derivative coefficients.
+template <typename F>
+void chebyshev_fit(int i, double r2min, double dx, F g_of_r2, double *o)
 {
   const double a = i * dx + r2min, b = (i + 1) * dx + r2min;
   double g[50], c[4];
   const double fac = 2.0 / 50;
   const double bma = 0.5 * (b - a), bpa = 0.5 * (b + a);
-  for (int k = 0; k < 50; k++) {
-    const double r2 = cos(M_PI * (k + 0.5) / 50) * bma + bpa;
-    const double r = sqrt(r2);
-    g[k] = erfc(eta * r) / r;
-  }
+  for (int k = 0; k < 50; k++)
+    g[k] = g_of_r2(cos(M_PI * (k + 0.5) / 50) * bma + bpa);
   for (int j = 0; j < 4; j++) {
     double s = 0;
     for (int k = 0; k < 50; k++)
@@ -76,6 +72,16 @@ void chebyshev_segment(int i, double r2min, double dx, double eta, double *o)
   o[4] = -2 * o[1] / (b - a);
   o[5] = -2 * 2 * o[2] / (b - a);
   o[6] = -2 * 3 * o[3] / (b - a);
+}
+
+// Segment i of the reference's erfc(eta r)/r table (src/rspace.c:18-37), same
+// formula and operation order: built on the host so segments 0..511 are
+// bitwise the ones RSpaceChebyshev_new builds.  Segments past 511 continue the
+// same construction beyond the reference's range (the rigid-water FP64 kernel
+// reads them for site pairs beyond 1.2 rc^2).
+void chebyshev_segment(int i, double r2min, double dx, double eta, double *o)
+{
+  chebyshev_fit(i, r2min, dx, [eta](double r2) { const double r = sqrt(r2); return erfc(eta * r) / r; }, o);
 }
 
 void chebyshev_table(double rhi, double eta, double *mn, double *mx, double *inv_dx, double *coeff7)
@@ -305,7 +311,20 @@ int setup_cheb(mmnb_handle *h)
     w[2 * ((size_t) h->cheb_w_nseg + i) + 1] = o[3];
   }
   h->water64_grid = 0;  // the kernel's shared-memory size follows the table
-  return upload(h, &h->d_cheb_w, w);
+  if ((s = upload(h, &h->d_cheb_w, w)))
+    return s;
+  // the same fit of (2 eta / sqrt(pi)) exp(-eta^2 r^2) = -eta d/d(eta) of
+  // erfc(eta r)/r: since the fit is linear in the sampled values, these cubics
+  // are exactly -eta d/d(eta) of the table's cubics (mmnb_virial's eta term)
+  std::vector<double> d4(4 * (size_t) kCheb);
+  const double eta = h->eta;
+  for (int i = 0; i < kCheb; i++) {
+    double o[7];
+    chebyshev_fit(i, h->cheb_min, dx, [eta](double r2) { return eta * M_2_SQRTPI * exp(-eta * eta * r2); }, o);
+    for (int k = 0; k < 4; k++)
+      d4[4 * i + k] = o[k];
+  }
+  return upload(h, &h->d_cheb_d, d4);
 }
 
 // reciprocal lattice 2 pi inv(latv)^T of the diagonal box
@@ -409,7 +428,8 @@ void free_all(mmnb_handle *h)
     h->ev_flags = nullptr;
   }
   void *ptrs[] = {h->d_group, h->d_excl_ptr, h->d_excl_idx, h->d_p14_ptr, h->d_p14_idx, h->d_gexcl_ptr,
-                  h->d_gexcl_idx, h->d_mask, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_cheb, h->d_cheb_w, h->d_lj_row,
+                  h->d_gexcl_idx, h->d_mask, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_cheb, h->d_cheb_w, h->d_cheb_d, h->d_lj_row,
+                  h->d_vir_part, h->d_vir_row, h->d_vir_mol, h->d_vir_molw, h->d_vir_mass,
                   h->d_stencil, h->d_cell_rank, h->d_cell_of_rank, h->d_cell_of_group, h->d_cell_count,
                   h->d_cell_start, h->d_slot, h->d_sorted, h->d_rank, h->d_anchor, h->d_last, h->d_anchor_sorted, h->d_anchor32, h->d_block_sum,
                   h->d_top2, h->d_nbr, h->d_nbr_count, h->d_pnbr, h->d_pcount, h->d_plast, h->d_flags, h->d_sr,
@@ -700,13 +720,14 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
   const size_t nlj = (size_t) h->lj_pair_blocks + h->lj_excl_blocks;
   if ((s = dalloc(h, &h->d_phi, nsite)) || (s = dalloc(h, &h->d_evec, 3 * (size_t) nsite)) ||
       (s = dalloc(h, &h->d_ljf, 3 * (size_t) nsite)) || (s = dalloc(h, &h->d_lj_part, nlj)) ||
-      (s = dalloc(h, &h->d_lj_row, ngroup)) ||
+      (s = dalloc(h, &h->d_lj_row, ngroup)) || (s = dalloc(h, &h->d_vir_part, nlj)) ||
+      (s = dalloc(h, &h->d_vir_row, ngroup)) ||
       (s = dalloc(h, &h->d_elec_part, h->elec_blocks)) || (s = dalloc(h, &h->d_energy, 8)) ||
       (s = dalloc(h, &h->d_r, 3 * (size_t) nsite)) || (s = dalloc(h, &h->d_f, 3 * (size_t) nsite)) ||
-      (s = dalloc(h, &h->d_wsum, 4)))
+      (s = dalloc(h, &h->d_wsum, 8)))
     return s;
   CK(cudaMemset(h->d_lj_part, 0, sizeof(double) * nlj));
-  CK(cudaMemset(h->d_wsum, 0, sizeof(unsigned long long) * 4));
+  CK(cudaMemset(h->d_wsum, 0, sizeof(unsigned long long) * 8));
   if (c->precision == MMNB_MIXED) {
     if ((s = dalloc(h, &h->mx.site, nslot)) || (s = dalloc(h, &h->mx.par, nslot)) ||
         (s = dalloc(h, &h->mx.anchor, ngroup)) ||
@@ -1028,7 +1049,7 @@ int mmnb_compute(mmnb_handle *h, const double *r, double *f, double *u, mmnb_ene
     CK(cudaMemcpyAsync(h->d_r, r, sizeof(double) * n3, cudaMemcpyHostToDevice, h->stream));
     // after the first call, a plain evaluation replays the handle's own graph
     // (zeroing, list check/rebuild, pair and mesh kernels, finalize)
-    const bool graph = !h->first && !(phi || evec) && !h->timing.on && !h->force_rebuild_next;
+    const bool graph = !h->first && !(phi || evec) && !h->timing.on && !h->force_rebuild_next && !h->want_virial;
     if (graph && !h->hgraph_exec) {
       CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
       h->capturing = true;

@@ -99,6 +99,7 @@ struct mmnb_handle {
   bool lj_on_anchors_only = false;   // every LJ site is its group's first site (rigid water)
   bool water = false;                // every group is [O(q, LJ), H(q), H(q)] with no screening or group exclusions
   bool want_fields = false;          // this evaluation must produce per-site potential and field
+  bool want_virial = false;          // this evaluation's pair kernels also sum the virial's pair term
   bool used_water = false;           // the last evaluation ran the water kernel
   bool used_water64 = false;         // the last evaluation ran the FP64 water kernel
   double totA = 0, totB = 0, lj_correction = 0, neutral_b = 0;
@@ -122,6 +123,8 @@ struct mmnb_handle {
   // the rigid-water FP64 kernel's table: cheb_w_nseg x (c0, c1), then x (c2, c3)
   double *d_cheb_w = nullptr;
   int cheb_w_nseg = 0;
+  // 512 x 4: the cubics of -eta d/d(eta) of the table (mmnb_virial)
+  double *d_cheb_d = nullptr;
   int water64_grid = 0;              // persistent blocks of that kernel (0: not sized yet)
   size_t water64_smem = 0;
 
@@ -172,8 +175,17 @@ struct mmnb_handle {
   double *d_phi = nullptr, *d_evec = nullptr, *d_ljf = nullptr;
   double *d_lj_part = nullptr;       // LJ energy partials: pair-kernel blocks, then exclusion blocks
   double *d_lj_row = nullptr;        // FP64 water kernel: LJ energy of each row (sorted order)
+  // mmnb_virial: the pair kernels' virial term (per block: pair-kernel blocks,
+  // then exclusion blocks; per row: FP64 water kernel), molecule ranges,
+  // masses and per-molecule sums (allocated on first use)
+  double *d_vir_part = nullptr, *d_vir_row = nullptr;
+  int *d_vir_mol = nullptr;
+  double *d_vir_molw = nullptr, *d_vir_mass = nullptr;
+  int vir_mol_cap = 0;
   // [0], [1]: fixed-point Coulomb and LJ pair energies of the water kernel;
-  // [2]: block counter of the finalize kernel's last-block reduction
+  // [2]: block counter of the finalize kernel's last-block reduction;
+  // [3]: row counter of the FP64 water kernel; [4]: the mixed water kernel's
+  // fixed-point virial term
   unsigned long long *d_wsum = nullptr;
   double *d_bwd = nullptr;           // backward pass: row partials and dL/dF (allocated on first use)
   size_t bwd_cap = 0;

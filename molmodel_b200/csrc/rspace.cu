@@ -43,10 +43,13 @@ struct PairArgs {
   const int *nbr, *nbr_count, *sorted, *group;
   const int *gexcl_ptr, *gexcl_idx, *excl_ptr, *excl_idx;
   double *phi, *evec, *ljf, *lj_part;
+  double *vir_part;  // per block: sum of the virial's pair term (mmnb_virial), or null
+  const double *cheb_d;  // 512 x 4: cubics of -eta d/d(eta) of the table (mmnb_virial)
 };
 
-// b0 = erfc(eta r)/r, b1 = (b0 + 2 eta/sqrt(pi) exp(-eta^2 r^2)) / r^2
-__device__ __forceinline__ void ewald_b(const PairArgs &a, double r2, double &b0, double &b1)
+// b0 = erfc(eta r)/r, b1 = (b0 + 2 eta/sqrt(pi) exp(-eta^2 r^2)) / r^2; seg and
+// f: the table segment and the position in it (seg = -1 outside the table)
+__device__ __forceinline__ void ewald_b(const PairArgs &a, double r2, double &b0, double &b1, int &seg, double &f)
 {
   if (a.cheb_min < r2 && r2 < a.cheb_max) {
     double x = (r2 - a.cheb_min) * a.cheb_inv_dx;
@@ -56,19 +59,36 @@ __device__ __forceinline__ void ewald_b(const PairArgs &a, double r2, double &b0
     x -= i;
     b0 = ((c23.y * x + c23.x) * x + c01.y) * x + c01.x;
     b1 = (c67.x * x + c45.y) * x + c45.x;
+    seg = (int) i;
+    f = x;
   } else {
     const double r = sqrt(r2);
     const double er = a.eta * r;
     const double e = exp(-(er * er));
     b0 = erfc(er) / r;
     b1 = (b0 + a.eta * M_2_SQRTPI * e) / r2;
+    seg = -1;
+    f = 0;
   }
+}
+
+// The table is refitted for each eta, so along the volume-move path its eta
+// derivative is the fitted cubic D of -eta d/d(eta) erfc(eta r)/r rather than
+// b1 r^2 - b0, the identity the exact function obeys and mmnb_virial's scale
+// covariance assumes: the difference, for the virial's pair term
+__device__ __forceinline__ double table_eta_term(const PairArgs &a, int seg, double f, double r2, double b0,
+                                                 double b1)
+{
+  const double2 *dc = reinterpret_cast<const double2 *>(a.cheb_d) + 2 * seg;
+  const double2 d01 = __ldg(dc), d23 = __ldg(dc + 1);
+  return ((d23.y * f + d23.x) * f + d01.y) * f + d01.x - (b1 * r2 - b0);
 }
 
 template <int G>
 struct PairAcc {
   double phi[G], ex[G], ey[G], ez[G], lx[G], ly[G], lz[G];
   double elj;
+  double vir;  // LJ and switch force scalars times r^2 (dU/ds terms the site forces do not carry)
 };
 
 // one group pair (row group i, partner slot q) inside the cutoff
@@ -123,8 +143,11 @@ __device__ __forceinline__ void pair_fp64(const PairArgs &a, const double4 (&ri)
         r2 = dx * dx + dy * dy + dz * dz;
       }
       if (m & MMNB_SITE_HAS_Q) {
-        double b0, b1;
-        ewald_b(a, r2, b0, b1);
+        double b0, b1, fseg;
+        int seg;
+        ewald_b(a, r2, b0, b1, seg, fseg);
+        if (a.vir_part && seg >= 0)
+          acc.vir -= 0.5 * ri[ia].w * rj[jb].w * s * table_eta_term(a, seg, fseg, r2, b0, b1);
         if (SCREEN) {
           const double rs = pi[ia].z + pj[jb].z;
           if (r2 < rs * rs) {
@@ -164,6 +187,7 @@ __device__ __forceinline__ void pair_fp64(const PairArgs &a, const double4 (&ri)
           du *= s;
         }
         acc.elj += 0.5 * u;
+        acc.vir += 0.5 * du * r2;
         acc.lx[ia] += du * dx;
         acc.ly[ia] += du * dy;
         acc.lz[ia] += du * dz;
@@ -174,6 +198,7 @@ __device__ __forceinline__ void pair_fp64(const PairArgs &a, const double4 (&ri)
     acc.lx[0] += ds * x * tmps;
     acc.ly[0] += ds * y * tmps;
     acc.lz[0] += ds * z * tmps;
+    acc.vir += 0.5 * ds * tmps * r2a;
   }
 }
 
@@ -184,7 +209,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, 3) k_pair_fp64(PairArgs a)
 {
   __shared__ double4 qsh[kPairWarps][kQueue];
   __shared__ int qix[kPairWarps][kQueue];
-  __shared__ double wlj[kPairWarps];
+  __shared__ double wlj[kPairWarps], wvir[kPairWarps];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int p = blockIdx.x * kPairWarps + w;
   PairAcc<G> acc;
@@ -192,6 +217,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, 3) k_pair_fp64(PairArgs a)
   for (int k = 0; k < G; k++)
     acc.phi[k] = acc.ex[k] = acc.ey[k] = acc.ez[k] = acc.lx[k] = acc.ly[k] = acc.lz[k] = 0;
   acc.elj = 0;
+  acc.vir = 0;
   if (p < a.ngroup) {
     double4 ri[G], pi[G];
     int mi[G];
@@ -253,6 +279,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, 3) k_pair_fp64(PairArgs a)
         acc.lz[k] += __shfl_xor_sync(0xffffffffu, acc.lz[k], off);
       }
       acc.elj += __shfl_xor_sync(0xffffffffu, acc.elj, off);
+      acc.vir += __shfl_xor_sync(0xffffffffu, acc.vir, off);
     }
     const int ns = a.group[2 * gi + 1] - si0;
 #pragma unroll
@@ -269,14 +296,20 @@ __global__ void __launch_bounds__(kPairWarps * 32, 3) k_pair_fp64(PairArgs a)
       }
     }
   }
-  if (lane == 0)
+  if (lane == 0) {
     wlj[w] = acc.elj;
+    wvir[w] = acc.vir;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double t = 0;
-    for (int k = 0; k < kPairWarps; k++)
+    double t = 0, v = 0;
+    for (int k = 0; k < kPairWarps; k++) {
       t += wlj[k];
+      v += wvir[k];
+    }
     a.lj_part[blockIdx.x] = t;
+    if (a.vir_part)
+      a.vir_part[blockIdx.x] = v;
   }
 }
 
@@ -316,6 +349,7 @@ struct ExclArgs {
   const int *mask, *excl_ptr, *excl_idx, *p14_ptr, *p14_idx;
   double *phi, *evec, *ljf;
   double *lj14_part;
+  double *vir14_part;  // per block: the 1-4 LJ force scalars times r^2 / 2 (mmnb_virial), or null
 };
 
 __device__ __forceinline__ void min_image_ref(const Box &b, double &x, double &y, double &z)
@@ -327,9 +361,9 @@ __device__ __forceinline__ void min_image_ref(const Box &b, double &x, double &y
 
 __global__ void __launch_bounds__(kExclThreads) k_exclusions_fp64(ExclArgs a)
 {
-  __shared__ double sl[kExclThreads];
+  __shared__ double sl[kExclThreads], sv[kExclThreads];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double elj = 0;
+  double elj = 0, vir = 0;
   if (i < a.nsite) {
     const int mi = a.mask[i];
     double phi = 0, ex = 0, ey = 0, ez = 0, lx = 0, ly = 0, lz = 0;
@@ -397,6 +431,7 @@ __global__ void __launch_bounds__(kExclThreads) k_exclusions_fp64(ExclArgs a)
             du *= a.l14;
           }
           elj += 0.5 * u;
+          vir += 0.5 * du * r2;
           lx += du * x;
           ly += du * y;
           lz += du * z;
@@ -425,14 +460,20 @@ __global__ void __launch_bounds__(kExclThreads) k_exclusions_fp64(ExclArgs a)
     }
   }
   sl[threadIdx.x] = elj;
+  sv[threadIdx.x] = vir;
   __syncthreads();
   for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s)
+    if (threadIdx.x < s) {
       sl[threadIdx.x] += sl[threadIdx.x + s];
+      sv[threadIdx.x] += sv[threadIdx.x + s];
+    }
     __syncthreads();
   }
-  if (threadIdx.x == 0)
+  if (threadIdx.x == 0) {
     a.lj14_part[blockIdx.x] = sl[0];
+    if (a.vir14_part)
+      a.vir14_part[blockIdx.x] = sv[0];
+  }
 }
 
 cudaError_t launch_sort_sites(mmnb_handle *h, const double *d_r)
@@ -495,6 +536,8 @@ cudaError_t launch_rspace_fp64(mmnb_handle *h)
   a.evec = h->d_evec;
   a.ljf = h->d_ljf;
   a.lj_part = h->d_lj_part;
+  a.vir_part = h->want_virial ? h->d_vir_part : nullptr;
+  a.cheb_d = h->d_cheb_d;
   switch (h->G) {
   case 1: launch_pair_g<1>(h, a); break;
   case 2: launch_pair_g<2>(h, a); break;
@@ -534,6 +577,7 @@ cudaError_t launch_exclusions(mmnb_handle *h, const double *d_r)
   a.evec = h->d_evec;
   a.ljf = h->d_ljf;
   a.lj14_part = h->d_lj_part + h->lj_pair_blocks;
+  a.vir14_part = h->want_virial ? h->d_vir_part + h->lj_pair_blocks : nullptr;
   k_exclusions_fp64<<<excl_blocks(h), kExclThreads, 0, h->stream>>>(a);
   h->launches += 1;
   return cudaGetLastError();

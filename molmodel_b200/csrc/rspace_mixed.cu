@@ -93,6 +93,7 @@ struct MixedArgs {
   const int *gexcl_ptr, *gexcl_idx, *excl_ptr, *excl_idx;
   long long *acc;               // per site, kAccStride
   double *lj_part;
+  double *vir_part;             // per block: the virial's pair term (mmnb_virial), or null
 };
 
 __device__ __forceinline__ long long to_fx(float v) { return __float2ll_rn(v * 4294967296.0f); }
@@ -100,7 +101,8 @@ __device__ __forceinline__ long long to_fx(float v) { return __float2ll_rn(v * 4
 // one group pair inside the cutoff: FP32 sums, then fixed point
 template <int G, bool SCREEN, bool GEXCL, bool ANCHOR_LJ>
 __device__ __forceinline__ void pair_mixed(const MixedArgs &a, const float4 (&oi)[G], const float4 (&pi)[G], int gi,
-                                           int si0, int q, float4 da, long long (&fx)[G][kNacc], long long &fe)
+                                           int si0, int q, float4 da, long long (&fx)[G][kNacc], long long &fe,
+                                           long long &fv)
 {
   float4 oj[G], pj[G];
 #pragma unroll
@@ -127,7 +129,7 @@ __device__ __forceinline__ void pair_mixed(const MixedArgs &a, const float4 (&oi
 #pragma unroll
   for (int k = 0; k < G; k++)
     ph[k] = ex[k] = ey[k] = ez[k] = lx[k] = ly[k] = lz[k] = 0.f;
-  float tmps = 0.f, u_sum = 0.f;
+  float tmps = 0.f, u_sum = 0.f, xv = 0.f;
 #pragma unroll
   for (int ia = 0; ia < G; ia++) {
     const int mi = __float_as_int(pi[ia].w);
@@ -176,6 +178,7 @@ __device__ __forceinline__ void pair_mixed(const MixedArgs &a, const float4 (&oi
         const float u = ai12 - bi6;
         tmps += u;
         u_sum = fmaf(u, s, u_sum);
+        xv = fmaf(du, r2, xv);
         lx[ia] = fmaf(du, dx, lx[ia]);
         ly[ia] = fmaf(du, dy, ly[ia]);
         lz[ia] = fmaf(du, dz, lz[ia]);
@@ -188,6 +191,7 @@ __device__ __forceinline__ void pair_mixed(const MixedArgs &a, const float4 (&oi
     lx[0] = fmaf(g, da.x, lx[0]);
     ly[0] = fmaf(g, da.y, ly[0]);
     lz[0] = fmaf(g, da.z, lz[0]);
+    xv = fmaf(g, r2a, xv);
   }
 #pragma unroll
   for (int k = 0; k < G; k++) {
@@ -202,6 +206,8 @@ __device__ __forceinline__ void pair_mixed(const MixedArgs &a, const float4 (&oi
     }
   }
   fe += to_fx(0.5f * u_sum);
+  if (a.vir_part)
+    fv += to_fx(0.5f * xv);
 }
 
 template <int G, bool SCREEN, bool GEXCL, bool ANCHOR_LJ>
@@ -209,10 +215,10 @@ __global__ void __launch_bounds__(kMxWarps * 32) k_pair_mixed(MixedArgs a)
 {
   __shared__ float4 qda[kMxWarps][kMxQueue];
   __shared__ int qix[kMxWarps][kMxQueue];
-  constexpr int kCols = G * kNacc + 1;
+  constexpr int kCols = G * kNacc + 2;  // site values, LJ energy, virial term
   constexpr bool kTranspose = G <= 4;
   __shared__ long long red[kTranspose ? kMxWarps : 1][kTranspose ? 32 : 1][kTranspose ? kCols : 1];
-  __shared__ long long wlj[kMxWarps];
+  __shared__ long long wlj[kMxWarps], wvir[kMxWarps];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int p = blockIdx.x * kMxWarps + w;
   long long fx[G][kNacc];
@@ -221,7 +227,7 @@ __global__ void __launch_bounds__(kMxWarps * 32) k_pair_mixed(MixedArgs a)
 #pragma unroll
     for (int c = 0; c < kNacc; c++)
       fx[k][c] = 0;
-  long long fe = 0;
+  long long fe = 0, fv = 0;
   int gi = 0, si0 = 0, ns = 0;
   if (p < a.ngroup) {
     float4 oi[G], pi[G];
@@ -259,7 +265,7 @@ __global__ void __launch_bounds__(kMxWarps * 32) k_pair_mixed(MixedArgs a)
       qn += __popc(bal);
       __syncwarp();
       if (qn >= 32) {
-        pair_mixed<G, SCREEN, GEXCL, ANCHOR_LJ>(a, oi, pi, gi, si0, qix[w][lane], qda[w][lane], fx, fe);
+        pair_mixed<G, SCREEN, GEXCL, ANCHOR_LJ>(a, oi, pi, gi, si0, qix[w][lane], qda[w][lane], fx, fe, fv);
         __syncwarp();
         if (lane < qn - 32) {
           qda[w][lane] = qda[w][lane + 32];
@@ -270,7 +276,7 @@ __global__ void __launch_bounds__(kMxWarps * 32) k_pair_mixed(MixedArgs a)
       }
     }
     if (lane < qn)
-      pair_mixed<G, SCREEN, GEXCL, ANCHOR_LJ>(a, oi, pi, gi, si0, qix[w][lane], qda[w][lane], fx, fe);
+      pair_mixed<G, SCREEN, GEXCL, ANCHOR_LJ>(a, oi, pi, gi, si0, qix[w][lane], qda[w][lane], fx, fe, fv);
   }
   if constexpr (kTranspose) {
     // transpose reduction: lane c sums column c over the 32 lanes
@@ -280,6 +286,7 @@ __global__ void __launch_bounds__(kMxWarps * 32) k_pair_mixed(MixedArgs a)
       for (int c = 0; c < kNacc; c++)
         red[w][lane][k * kNacc + c] = fx[k][c];
     red[w][lane][G * kNacc] = fe;
+    red[w][lane][G * kNacc + 1] = fv;
     __syncwarp();
     for (int c = lane; c < kCols; c += 32) {
       long long t = 0;
@@ -287,6 +294,8 @@ __global__ void __launch_bounds__(kMxWarps * 32) k_pair_mixed(MixedArgs a)
         t += red[w][l][c];
       if (c == G * kNacc) {
         wlj[w] = t;
+      } else if (c == G * kNacc + 1) {
+        wvir[w] = t;
       } else if (p < a.ngroup) {
         const int k = c / kNacc, comp = c % kNacc;
         if (k < ns)
@@ -302,9 +311,12 @@ __global__ void __launch_bounds__(kMxWarps * 32) k_pair_mixed(MixedArgs a)
         for (int c = 0; c < kNacc; c++)
           fx[k][c] += __shfl_xor_sync(0xffffffffu, fx[k][c], off);
       fe += __shfl_xor_sync(0xffffffffu, fe, off);
+      fv += __shfl_xor_sync(0xffffffffu, fv, off);
     }
-    if (lane == 0)
+    if (lane == 0) {
       wlj[w] = fe;
+      wvir[w] = fv;
+    }
     if (p < a.ngroup)
 #pragma unroll
       for (int k = 0; k < G; k++)
@@ -315,10 +327,14 @@ __global__ void __launch_bounds__(kMxWarps * 32) k_pair_mixed(MixedArgs a)
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    long long t = 0;
-    for (int k = 0; k < kMxWarps; k++)
+    long long t = 0, v = 0;
+    for (int k = 0; k < kMxWarps; k++) {
       t += wlj[k];
+      v += wvir[k];
+    }
     a.lj_part[blockIdx.x] = (double) t * kFxInv;
+    if (a.vir_part)
+      a.vir_part[blockIdx.x] = (double) v * kFxInv;
   }
 }
 
@@ -367,7 +383,8 @@ struct WaterArgs {
   const double4 *anchor;
   const int *nbr, *nbr_count, *sorted, *group;
   long long *acc;         // per site: slots 4..6 receive the force, 0..3 are cleared
-  unsigned long long *wsum;  // fixed-point Coulomb and LJ pair energies, zeroed by the prep kernel
+  unsigned long long *wsum;  // fixed-point Coulomb and LJ pair energies and, with the virial,
+                             // the virial's pair term (wsum[4]); zeroed by the prep kernel
   // pruned rows (null: none): read when flags[kFlagPruneFull] is 0; made from
   // the full rows (pairs with r^2 <= rp2) when it is 1
   int *pnbr, *pcount;
@@ -518,13 +535,15 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // MINB: resident warps per SM / 4 the register budget is cut for (4: 128
 // registers, 5: 96); mmnb_autotune picks per handle
-template <int MINB>
+// VIR: also the part of dU/ds (box scaling) the site forces do not carry, the
+// anchor force scalar times R^2 per group pair (mmnb_virial)
+template <int MINB, bool VIR>
 __global__ void __launch_bounds__(kWaterWarps * 32, MINB * kMxWarps / kWaterWarps) k_pair_water(WaterArgs a)
 {
   // per warp: ring of anchor displacement (xyz, r^2) and the partner's three
   // packed slots
   __shared__ float4 ring[kWaterWarps][4][kWaterRing];
-  constexpr int kCols = 11;
+  constexpr int kCols = VIR ? 12 : 11;
   constexpr int kMask = kWaterRing - 1;
   constexpr float kTwo32 = 4294967296.0f, kTwo31 = 2147483648.0f;
   long long fx[kCols];
@@ -636,6 +655,8 @@ __global__ void __launch_bounds__(kWaterWarps * 32, MINB * kMxWarps / kWaterWarp
       fx[8] += __float2ll_rn(qH2_32 * e2z);
       fx[9] += __float2ll_rn(tq * s31);
       fx[10] += __float2ll_rn(u * s31);
+      if constexpr (VIR)
+        fx[11] += __float2ll_rn(0.5f * fo32 * da.w);  // each pair is seen from both rows
     };
     // Entries past the row end read the row's own group (a valid address);
     // they are never accepted.
@@ -697,7 +718,7 @@ __global__ void __launch_bounds__(kWaterWarps * 32, MINB * kMxWarps / kWaterWarp
   }
   if (a.pnbr && a.flags[kFlagPruneFull] && blockIdx.x == 0 && threadIdx.x == 0)
     a.flags[kFlagPruneValid] = 1;
-  __shared__ long long wsum[kWaterWarps][2];
+  __shared__ long long wsum[kWaterWarps][3];
   // lane totals, transposed through the warp's own ring (no longer in use)
   static_assert(32 * (kCols + 1) * sizeof(long long) <= sizeof(ring[0]), "ring too small for the reduction");
   long long(*red)[kCols + 1] = reinterpret_cast<long long(*)[kCols + 1]>(ring[w]);
@@ -716,21 +737,25 @@ __global__ void __launch_bounds__(kWaterWarps * 32, MINB * kMxWarps / kWaterWarp
     } else {
       wsum[w][lane - 9] = t;
     }
-  } else if (lane < 11 + 12 && p < a.ngroup) {
+  } else if (lane < kCols + 12 && p < a.ngroup) {
     // clear the potential and field slots of the three sites (P3M adds to them)
-    const int k = lane - 11;
+    const int k = lane - kCols;
     a.acc[(size_t) (si0 + k / 4) * kAccStride + k % 4] = 0;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    long long te = 0, tl = 0;
+    long long te = 0, tl = 0, tv = 0;
     for (int k = 0; k < kWaterWarps; k++) {
       te += wsum[k][0];
       tl += wsum[k][1];
+      if (VIR)
+        tv += wsum[k][2];
     }
     // integer sums: the totals do not depend on the order blocks finish in
     atomicAdd(a.wsum, (unsigned long long) te);
     atomicAdd(a.wsum + 1, (unsigned long long) tl);
+    if (VIR)
+      atomicAdd(a.wsum + 4, (unsigned long long) tv);
   }
 }
 
@@ -761,10 +786,12 @@ cudaError_t launch_rspace_water(mmnb_handle *h)
   a.flags = h->d_flags;
   a.rp2 = (h->rc + h->prune_margin) * (h->rc + h->prune_margin);
   const int blocks = div_up(h->ngroup, kWaterWarps);
-  if (h->tune.water_minb == 5)
-    k_pair_water<5><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
+  if (h->want_virial)
+    k_pair_water<4, true><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
+  else if (h->tune.water_minb == 5)
+    k_pair_water<5, false><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
   else
-    k_pair_water<4><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
+    k_pair_water<4, false><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
   h->launches += 1;
   return cudaGetLastError();
 }
@@ -784,6 +811,8 @@ __global__ void k_prep_mixed(const double *__restrict__ r, const double *__restr
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < 2)
     wsum[s] = 0ull;
+  if (s == 2)
+    wsum[4] = 0ull;
   if (s >= ngroup * G)
     return;
   const int p = s / G, k = s % G;
@@ -873,6 +902,7 @@ cudaError_t launch_rspace_mixed(mmnb_handle *h)
   a.excl_idx = h->d_excl_idx;
   a.acc = h->mx.acc;
   a.lj_part = h->d_lj_part;
+  a.vir_part = h->want_virial ? h->d_vir_part : nullptr;
   const bool alj = h->lj_on_anchors_only;
   switch (h->G) {
   case 1: launch_mixed_g<1, false>(h, a); break;

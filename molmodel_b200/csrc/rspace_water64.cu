@@ -47,7 +47,7 @@ constexpr int kW64Warps = MMNB_W64_WARPS;
 // a batch of 32 is queued before the oldest 32 are evaluated, so the ring
 // holds up to 63 + 32 entries
 constexpr int kW64Ring = 128;
-constexpr int kW64Acc = 16;  // phi (3), field (9), LJ + switch force on O (3), LJ energy
+constexpr int kW64Acc = 17;  // phi (3), field (9), LJ + switch force on O (3), LJ energy, virial term
 
 struct Water64Args {
   int ngroup, rowcap, geometric, nseg;
@@ -60,22 +60,28 @@ struct Water64Args {
   const int *nbr, *nbr_count, *sorted, *group;
   unsigned long long *counter;         // next row; zeroed by k_sort_water64
   double *phi, *evec, *ljf, *lj_row;
+  double *vir_row;                     // per row: the virial's pair term (mmnb_virial), or null
+  const double *cheb_d;                // 512 x 4: cubics of -eta d/d(eta) of the table (mmnb_virial)
 };
 
-// b0 = erfc(eta r)/r and b1 = (b0 + 2 eta/sqrt(pi) exp(-eta^2 r^2)) / r^2
+// b0 = erfc(eta r)/r and b1 = (b0 + 2 eta/sqrt(pi) exp(-eta^2 r^2)) / r^2;
+// seg and f: the table segment and the position in it, seg = -1 outside the table
 __device__ __forceinline__ void ewald_w64(const Water64Args &a, const double2 *t0, const double2 *t1, double r2,
-                                          double &b0, double &b1)
+                                          double &b0, double &b1, int &seg, double &f)
 {
   const double x = (r2 - a.cmin) * a.inv_dx;
   if (x > 0 && x < a.nsegd) {
     // floor(x) exactly: x + 2^52 rounded down holds floor(x) in its low word
     const double t = __dadd_rd(x, 4503599627370496.0);
     const int i = __double2loint(t);
-    const double f = x - (t - 4503599627370496.0);
+    f = x - (t - 4503599627370496.0);
+    seg = i;
     const double2 c01 = t0[i], c23 = t1[i];
     b0 = ((c23.y * f + c23.x) * f + c01.y) * f + c01.x;
     b1 = a.dscale * ((3 * c23.y * f + 2 * c23.x) * f + c01.y);
   } else {
+    seg = -1;
+    f = 0;
     const double r = sqrt(r2);
     const double er = a.eta * r;
     b0 = erfc(er) / r;
@@ -83,19 +89,32 @@ __device__ __forceinline__ void ewald_w64(const Water64Args &a, const double2 *t
   }
 }
 
-// one site pair: d = displacement, qj = partner charge, qjs = qj S
+// one site pair: d = displacement, qj = partner charge, qjs = qj S.
+// VIR: the site pair's part of the virial that scale covariance misses --
+// the table is refitted for each eta, so its eta derivative is the fitted
+// cubic D of -eta d/d(eta) erfc(eta r)/r, not b1 r^2 - b0 (the identity the
+// exact function obeys); qis = q_i S, added to the virial term with the
+// factor -1/2 (the full list sees each pair twice)
+template <bool VIR>
 __device__ __forceinline__ void site_w64(const Water64Args &a, const double2 *t0, const double2 *t1, double dx,
                                          double dy, double dz, double r2, double qj, double qjs, double &ph,
-                                         double &ex, double &ey, double &ez, double &tq)
+                                         double &ex, double &ey, double &ez, double &tq, double qis, double &vir)
 {
-  double b0, b1;
-  ewald_w64(a, t0, t1, r2, b0, b1);
+  double b0, b1, f;
+  int seg;
+  ewald_w64(a, t0, t1, r2, b0, b1, seg, f);
   tq += qj * b0;
   ph += qjs * b0;
-  const double f = qjs * b1;
-  ex += f * dx;
-  ey += f * dy;
-  ez += f * dz;
+  const double fb = qjs * b1;
+  ex += fb * dx;
+  ey += fb * dy;
+  ez += fb * dz;
+  if (VIR && seg >= 0 && seg < kCheb) {
+    const double2 *dc = reinterpret_cast<const double2 *>(a.cheb_d) + 2 * seg;
+    const double2 d01 = __ldg(dc), d23 = __ldg(dc + 1);
+    const double dd = ((d23.y * f + d23.x) * f + d01.y) * f + d01.x;
+    vir -= 0.5 * qis * qj * (dd - (b1 * r2 - b0));
+  }
 }
 
 __device__ __forceinline__ void cp16(void *dst, const void *src)
@@ -105,6 +124,7 @@ __device__ __forceinline__ void cp16(void *dst, const void *src)
                : "memory");
 }
 
+template <bool VIR>
 __global__ void __launch_bounds__(kW64Warps * 32, MMNB_W64_BLOCKS) k_pair_water64(Water64Args a)
 {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -144,38 +164,39 @@ __global__ void __launch_bounds__(kW64Warps * 32, MMNB_W64_BLOCKS) k_pair_water6
       const double s = ((-6 * zz + 15) * zz - 10) * zz * zz * zz + 1;
       const double ds = ((60 * zz - 120) * zz + 60) * zz * zz * a.inv_sw;
       const double qjOs = qjO * s, qj1s = qj1 * s, qj2s = qj2 * s;
+      const double qOs = qO * s, qH1s = qH1 * s, qH2s = qH2 * s;
       double tO = 0, t1 = 0, t2 = 0;
       // row O
-      site_w64(a, tc01, tc23, da.x, da.y, da.z, r2a, qjO, qjOs, acc[0], acc[3], acc[4], acc[5], tO);
+      site_w64<VIR>(a, tc01, tc23, da.x, da.y, da.z, r2a, qjO, qjOs, acc[0], acc[3], acc[4], acc[5], tO, qOs, acc[16]);
       {
         const double dx = da.x - j1x, dy = da.y - j1y, dz = da.z - j1z;
-        site_w64(a, tc01, tc23, dx, dy, dz, dx * dx + dy * dy + dz * dz, qj1, qj1s, acc[0], acc[3], acc[4], acc[5], tO);
+        site_w64<VIR>(a, tc01, tc23, dx, dy, dz, dx * dx + dy * dy + dz * dz, qj1, qj1s, acc[0], acc[3], acc[4], acc[5], tO, qOs, acc[16]);
       }
       {
         const double dx = da.x - j2x, dy = da.y - j2y, dz = da.z - j2z;
-        site_w64(a, tc01, tc23, dx, dy, dz, dx * dx + dy * dy + dz * dz, qj2, qj2s, acc[0], acc[3], acc[4], acc[5], tO);
+        site_w64<VIR>(a, tc01, tc23, dx, dy, dz, dx * dx + dy * dy + dz * dz, qj2, qj2s, acc[0], acc[3], acc[4], acc[5], tO, qOs, acc[16]);
       }
       // row H1
       {
         const double cx = da.x + h1x, cy = da.y + h1y, cz = da.z + h1z;
-        site_w64(a, tc01, tc23, cx, cy, cz, cx * cx + cy * cy + cz * cz, qjO, qjOs, acc[1], acc[6], acc[7], acc[8], t1);
+        site_w64<VIR>(a, tc01, tc23, cx, cy, cz, cx * cx + cy * cy + cz * cz, qjO, qjOs, acc[1], acc[6], acc[7], acc[8], t1, qH1s, acc[16]);
         double dx = cx - j1x, dy = cy - j1y, dz = cz - j1z;
-        site_w64(a, tc01, tc23, dx, dy, dz, dx * dx + dy * dy + dz * dz, qj1, qj1s, acc[1], acc[6], acc[7], acc[8], t1);
+        site_w64<VIR>(a, tc01, tc23, dx, dy, dz, dx * dx + dy * dy + dz * dz, qj1, qj1s, acc[1], acc[6], acc[7], acc[8], t1, qH1s, acc[16]);
         dx = cx - j2x;
         dy = cy - j2y;
         dz = cz - j2z;
-        site_w64(a, tc01, tc23, dx, dy, dz, dx * dx + dy * dy + dz * dz, qj2, qj2s, acc[1], acc[6], acc[7], acc[8], t1);
+        site_w64<VIR>(a, tc01, tc23, dx, dy, dz, dx * dx + dy * dy + dz * dz, qj2, qj2s, acc[1], acc[6], acc[7], acc[8], t1, qH1s, acc[16]);
       }
       // row H2
       {
         const double cx = da.x + h2x, cy = da.y + h2y, cz = da.z + h2z;
-        site_w64(a, tc01, tc23, cx, cy, cz, cx * cx + cy * cy + cz * cz, qjO, qjOs, acc[2], acc[9], acc[10], acc[11], t2);
+        site_w64<VIR>(a, tc01, tc23, cx, cy, cz, cx * cx + cy * cy + cz * cz, qjO, qjOs, acc[2], acc[9], acc[10], acc[11], t2, qH2s, acc[16]);
         double dx = cx - j1x, dy = cy - j1y, dz = cz - j1z;
-        site_w64(a, tc01, tc23, dx, dy, dz, dx * dx + dy * dy + dz * dz, qj1, qj1s, acc[2], acc[9], acc[10], acc[11], t2);
+        site_w64<VIR>(a, tc01, tc23, dx, dy, dz, dx * dx + dy * dy + dz * dz, qj1, qj1s, acc[2], acc[9], acc[10], acc[11], t2, qH2s, acc[16]);
         dx = cx - j2x;
         dy = cy - j2y;
         dz = cz - j2z;
-        site_w64(a, tc01, tc23, dx, dy, dz, dx * dx + dy * dy + dz * dz, qj2, qj2s, acc[2], acc[9], acc[10], acc[11], t2);
+        site_w64<VIR>(a, tc01, tc23, dx, dy, dz, dx * dx + dy * dy + dz * dz, qj2, qj2s, acc[2], acc[9], acc[10], acc[11], t2, qH2s, acc[16]);
       }
       // O-O Lennard-Jones (src/rspace.c:258-297)
       const double sg = a.geometric ? sgO * sgj : (0.5 * (sgO + sgj)) * (0.5 * (sgO + sgj));
@@ -194,6 +215,9 @@ __global__ void __launch_bounds__(kW64Warps * 32, MMNB_W64_BLOCKS) k_pair_water6
       acc[12] += g * da.x;
       acc[13] += g * da.y;
       acc[14] += g * da.z;
+      // the part of dU/ds (box scaling) the site forces do not carry: the LJ and
+      // switch force scalar times R^2 (each pair is seen from both rows: half)
+      acc[16] += 0.5 * g * r2a;
     };
     const int cnt = a.nbr_count[p];
     const int *row = a.nbr + (size_t) p * a.rowcap;
@@ -261,8 +285,10 @@ __global__ void __launch_bounds__(kW64Warps * 32, MMNB_W64_BLOCKS) k_pair_water6
         a.evec[3 * si0 + (lane - 3)] = t;
       else if (lane < 15)
         a.ljf[3 * si0 + (lane - 12)] = t;
-      else
+      else if (lane == 15)
         a.lj_row[p] = t;
+      else if (a.vir_row)
+        a.vir_row[p] = t;
     } else if (lane < kW64Acc + 6) {
       // the H sites carry no LJ force
       a.ljf[3 * si0 + 3 + (lane - kW64Acc)] = 0;
@@ -312,14 +338,19 @@ cudaError_t launch_rspace_water64(mmnb_handle *h)
   const size_t smem = water64_smem(h);
   if (h->water64_grid == 0) {
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_pair_water64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)) !=
-        cudaSuccess)
+    if ((e = cudaFuncSetAttribute(k_pair_water64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)) !=
+            cudaSuccess ||
+        (e = cudaFuncSetAttribute(k_pair_water64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)) !=
+            cudaSuccess)
       return e;
-    int per_sm = 0, nsm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_water64, kW64Warps * 32, smem)) !=
+    int per_sm = 0, per_sm_v = 0, nsm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_water64<false>, kW64Warps * 32, smem)) !=
+            cudaSuccess ||
+        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_v, k_pair_water64<true>, kW64Warps * 32, smem)) !=
             cudaSuccess ||
         (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->dev)) != cudaSuccess)
       return e;
+    per_sm = std::min(per_sm, per_sm_v);
     if (per_sm < 1)
       return cudaErrorLaunchOutOfResources;
     h->water64_grid = std::min(per_sm * nsm, div_up(h->ngroup, kW64Warps));
@@ -351,7 +382,12 @@ cudaError_t launch_rspace_water64(mmnb_handle *h)
   a.evec = h->d_evec;
   a.ljf = h->d_ljf;
   a.lj_row = h->d_lj_row;
-  k_pair_water64<<<h->water64_grid, kW64Warps * 32, h->water64_smem, h->stream>>>(a);
+  a.vir_row = h->want_virial ? h->d_vir_row : nullptr;
+  a.cheb_d = h->d_cheb_d;
+  if (h->want_virial)
+    k_pair_water64<true><<<h->water64_grid, kW64Warps * 32, h->water64_smem, h->stream>>>(a);
+  else
+    k_pair_water64<false><<<h->water64_grid, kW64Warps * 32, h->water64_smem, h->stream>>>(a);
   h->launches += 1;
   return cudaGetLastError();
 }

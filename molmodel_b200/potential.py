@@ -102,6 +102,7 @@ class ElecLJ:
         if st:
             raise _lib.MmnbError(st, lib.mmnb_last_error(None).decode())
         self._h = h
+        self._groups = groups
         self.nsite = int(system.nsite)
         self.set_params(system.site_mask, system.q, system.sigma, system.epsilon, system.rscreen)
         return self
@@ -156,6 +157,22 @@ class ElecLJ:
         check(lib.mmnb_compute(self._h, _d(r), _d(f), ctypes.byref(uu), ctypes.byref(e), None, None), self._h)
         self.energy = dict(elec=e.elec, lj=e.lj, lj_correction=e.lj_correction, total=e.total)
         return uu.value
+
+    def virial(self, r, masses, molecules=None):
+        """dU/ds at s = 1 along the reference's volume-move path (mmnb_virial):
+        box x s, each molecule moved rigidly so its centre of mass is x s,
+        eta / s.  ``molecules``: (nmol, 2) half-open site ranges (default: the
+        groups).  Returns (w, energy dict, forces)."""
+        lib = load()
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        m = np.ascontiguousarray(masses, dtype=np.float64)
+        mol = np.ascontiguousarray(self._groups if molecules is None else molecules, dtype=np.int32)
+        f = np.zeros((self.nsite, 3))
+        e = MmnbEnergy()
+        w = ctypes.c_double(0.0)
+        check(lib.mmnb_virial(self._h, _d(r), len(mol), _i(mol), _d(m), _d(f), None, ctypes.byref(e),
+                              ctypes.byref(w)), self._h)
+        return w.value, dict(elec=e.elec, lj=e.lj, lj_correction=e.lj_correction, total=e.total), f
 
     def autotune(self, r, iters=10):
         """Time the launch choices at positions r and keep the fastest;
