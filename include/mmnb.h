@@ -158,7 +158,10 @@ int mmnb_graph_capture(mmnb_handle *h, const double *d_r, double *d_f, double *d
 int mmnb_graph_launch(mmnb_handle *h);
 
 /* Volume move by factor s: box, eta /= s, Chebyshev table, influence function
-   and cell stencil follow (src/eleclj.cpp:1268-1280, src/pppm.c:643-664). */
+   and cell stencil follow (src/eleclj.cpp:1268-1280, src/pppm.c:643-664).
+   MMNB_ERR_CUTOFF, with the handle unchanged, when the scaled box would no
+   longer hold the cutoff (rc > 0.49 x smallest edge, ElecLJ::init's rule,
+   src/eleclj.cpp:168-182) or rc + neighbour-list width would reach half of it. */
 int mmnb_scale(mmnb_handle *h, double s);
 
 /* Bind the handle to a CUDA stream (cudaStream_t passed as void*). */
@@ -177,6 +180,26 @@ int mmnb_get_cells(mmnb_handle *h, int *cell_of_group, int *ncell_per_dim);
 
 /* Number of list rebuilds so far and number of evaluations. */
 int mmnb_get_counters(mmnb_handle *h, long *rebuilds, long *evaluations);
+
+/* Status of the evaluations since the last check, for callers that evaluate
+   on device arrays (mmnb_compute_device, mmnb_graph_launch and graphs of their
+   own): synchronises the handle's stream.  The reference has no such state --
+   its neighbour rows grow on the host as they fill (src/pbin.c:41-50) and its
+   errors call die() -- so this reports, after the fact, what the device path
+   met:
+     MMNB_ERR_OVERFLOW  evaluations (their number in *truncated) ran on
+                        neighbour rows cut at their capacity, so pairs were
+                        missing; the rows are regrown and the next evaluation
+                        rebuilds the list.  Graphs captured before hold the old
+                        rows: mmnb_graph_launch refuses them until captured
+                        again, and the MD integrators capture again themselves;
+     MMNB_ERR_DEVICE    a site coordinate was not finite (NaN or infinite);
+     MMNB_OK            neither.
+   max_row receives the longest row needed.  Both conditions are cleared.
+   mmnb_compute checks them itself (it grows the rows and evaluates again, or
+   returns MMNB_ERR_DEVICE without adding to f or u); mmnb_md_run and
+   mmnb_md_batch_run return this status for their runs. */
+int mmnb_check(mmnb_handle *h, long *truncated, int *max_row);
 
 /* Number of this library's kernels launched on the handle's stream so far
    (library kernels such as cuFFT's are not counted). */
@@ -319,8 +342,10 @@ int mmnb_md_create(mmnb_handle *h, const double *site_mass, double dt, int rigid
    Velocities are projected onto the constraints and the forces evaluated. */
 int mmnb_md_set_state(mmnb_md *md, const double *r, const double *v);
 /* nsteps steps; energies (3*nsteps: kinetic, potential, conserved per step)
-   may be NULL.  MMNB_ERR_OVERFLOW when a neighbour row outgrew its capacity
-   during the run. */
+   may be NULL.  Returns mmnb_check's status for the run: MMNB_ERR_OVERFLOW
+   when a neighbour row outgrew its capacity during the run (the rows are
+   regrown, so running again from a saved state gives complete rows),
+   MMNB_ERR_DEVICE for a non-finite coordinate. */
 int mmnb_md_run(mmnb_md *md, int nsteps, double *energies);
 int mmnb_md_get_state(mmnb_md *md, double *r, double *v);
 const char *mmnb_md_last_error(const mmnb_md *md);

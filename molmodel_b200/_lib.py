@@ -71,6 +71,7 @@ SIGNATURES = [
     ("mmnb_get_cells", ctypes.c_int, [_vp, _ip, _ip]),
     ("mmnb_get_counters", ctypes.c_int, [_vp, _lp, _lp]),
     ("mmnb_get_launches", ctypes.c_int, [_vp, _lp]),
+    ("mmnb_check", ctypes.c_int, [_vp, _lp, _ip]),
     ("mmnb_get_settings", ctypes.c_int, [_vp, _dp, _dp, _dp, _ip]),
     ("mmnb_set_timing", ctypes.c_int, [_vp, ctypes.c_int]),
     ("mmnb_get_timing", ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),

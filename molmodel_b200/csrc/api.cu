@@ -127,6 +127,7 @@ unsigned spread_bits(unsigned v)
 template <typename T>
 int dalloc(mmnb_handle *h, T **p, size_t n)
 {
+  h->buf_gen++;
   if (*p) {
     cudaFree(*p);
     *p = nullptr;
@@ -798,6 +799,7 @@ int mmnb_set_params(mmnb_handle *h, const int *site_mask, const double *q, const
   if (!h || !site_mask || !q || !sig || !eps)
     return fail(h, MMNB_ERR_ARG, "null parameter array");
   drop_host_graph(h);
+  h->buf_gen++;  // the kernels an evaluation launches may change
   const int n = h->nsite;
   std::vector<double> rs(n, 0.0);
   h->any_q = h->any_lj = h->has_rscreen = false;
@@ -1010,6 +1012,7 @@ int mmnb_graph_capture(mmnb_handle *h, const double *d_r, double *d_f, double *d
     return fail(h, MMNB_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
   h->graph = g;
   CK(cudaGraphInstantiate(&h->graph_exec, h->graph, cudaGraphInstantiateFlagUseNodePriority));
+  h->graph_gen = h->buf_gen;
   return MMNB_OK;
 }
 
@@ -1017,6 +1020,10 @@ int mmnb_graph_launch(mmnb_handle *h)
 {
   if (!h || !h->graph_exec)
     return fail(h, MMNB_ERR_STATE, "no captured evaluation");
+  if (h->graph_gen != h->buf_gen)
+    return fail(h, MMNB_ERR_STATE,
+                "device buffers were reallocated since the capture (rows regrown, mmnb_scale, mmnb_set_params): "
+                "capture again");
   CK(cudaGraphLaunch(h->graph_exec, h->stream));
   h->evals++;
   h->launches += h->launch_per_eval;
@@ -1106,9 +1113,21 @@ int mmnb_compute(mmnb_handle *h, const double *r, double *f, double *u, mmnb_ene
       CK(cudaMemcpyAsync(evec, h->d_evec, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaEventSynchronize(h->ev_flags));
     h->rebuilds = h->h_flags[5];
-    if (h->h_flags[kFlagOverflow] > 0) {
-      // a row outgrew its capacity: grow, force a rebuild, evaluate again
+    if (h->h_flags[kFlagError]) {
+      // a device-side check failed (non-finite site coordinates): nothing is
+      // added to f or u, the flag is cleared and the handle stays usable
       CK(cudaStreamSynchronize(h->stream));
+      CK(cudaMemsetAsync(h->d_flags + kFlagError, 0, sizeof(int), h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+      return fail(h, MMNB_ERR_DEVICE, "a site coordinate is not finite (NaN or infinite)");
+    }
+    if (h->h_flags[kFlagOverflow] > 0) {
+      // a row outgrew its capacity: grow, force a rebuild, evaluate again (the
+      // evaluation on cut rows is not returned, so it is not counted either)
+      CK(cudaStreamSynchronize(h->stream));
+      h->h_flags[kFlagTruncEvals] -= 1;
+      CK(cudaMemcpy(h->d_flags + kFlagTruncEvals, h->h_flags + kFlagTruncEvals, sizeof(int),
+                    cudaMemcpyHostToDevice));
       const int need = h->h_flags[kFlagOverflow];
       int st = alloc_rows(h, (need + need / 4 + 63) / 32 * 32);
       if (st)
@@ -1152,6 +1171,18 @@ int mmnb_scale(mmnb_handle *h, double s)
 {
   if (!h || !(s > 0))
     return fail(h, MMNB_ERR_ARG, "scale factor must be > 0");
+  {
+    // the scaled box must still hold the cutoff (ElecLJ::init's rule,
+    // src/eleclj.cpp:168-182) and the listed range within half its smallest
+    // edge (minimum image); refused with the handle unchanged
+    const double dmin = s * h->min_diameter;
+    if (h->rc > 0.49 * dmin)
+      return fail(h, MMNB_ERR_CUTOFF, "after scaling by " + std::to_string(s) +
+                                          ", rspace_cutoff would exceed 0.49 * minimum diameter of box");
+    if (h->rc + h->nlw >= 0.5 * dmin)
+      return fail(h, MMNB_ERR_CUTOFF, "after scaling by " + std::to_string(s) +
+                                          ", rspace_cutoff + neighbor_list_width would reach half the box");
+  }
   drop_host_graph(h);
   for (int d = 0; d < 3; d++) {
     h->box.L[d] *= s;
@@ -1256,6 +1287,42 @@ int mmnb_get_counters(mmnb_handle *h, long *rebuilds, long *evaluations)
     *rebuilds = fl[5];
   if (evaluations)
     *evaluations = fl[4];
+  return MMNB_OK;
+}
+
+int mmnb_check(mmnb_handle *h, long *truncated, int *max_row)
+{
+  if (!h)
+    return MMNB_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  int fl[kFlagCount];
+  CK(cudaMemcpy(fl, h->d_flags, sizeof(fl), cudaMemcpyDeviceToHost));
+  if (truncated)
+    *truncated = fl[kFlagTruncEvals];
+  if (max_row)
+    *max_row = std::max(fl[kFlagMaxRow], fl[kFlagOverflow]);
+  // cleared for the next period; the sticky longest-row record stays
+  const int zero[2] = {0, 0};
+  CK(cudaMemcpy(h->d_flags + kFlagError, zero, sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_flags + kFlagTruncEvals, zero, sizeof(int), cudaMemcpyHostToDevice));
+  if (fl[kFlagError])
+    return fail(h, MMNB_ERR_DEVICE, "a site coordinate was not finite (NaN or infinite) in an evaluation");
+  if (fl[kFlagTruncEvals] > 0) {
+    // grow the rows and rebuild at the next evaluation; graphs captured before
+    // hold the old rows and are refused until captured again
+    const int need = std::max(fl[kFlagOverflow], fl[kFlagMaxRow]);
+    int st = alloc_rows(h, (need + need / 4 + 63) / 32 * 32);
+    if (st)
+      return st;
+    CK(cudaMemcpy(h->d_flags + kFlagOverflow, zero, sizeof(int), cudaMemcpyHostToDevice));
+    // a device-side request, so a graph captured after this does not carry it
+    const int one = 1;
+    CK(cudaMemcpy(h->d_flags + kFlagForceRebuild, &one, sizeof(int), cudaMemcpyHostToDevice));
+    return fail(h, MMNB_ERR_OVERFLOW,
+                std::to_string(fl[kFlagTruncEvals]) + " evaluation(s) ran on neighbour rows cut at their capacity (" +
+                    std::to_string(need) + " entries needed); the rows have been regrown and the next evaluation "
+                    "rebuilds the list");
+  }
   return MMNB_OK;
 }
 

@@ -28,6 +28,7 @@ struct FinArgs {
   int nrow;
   const unsigned long long *wsum;     // water kernel's fixed-point pair energies, or null
   unsigned long long *counter;        // finished-block counter, left at 0
+  int *flags;                         // list flags: counts evaluations finished on cut rows
   double tail;
   double *energy;
 };
@@ -131,6 +132,8 @@ __global__ void __launch_bounds__(kFinThreads) k_finalize(FinArgs a)
     a.energy[2] = a.tail;
     a.energy[3] = elec + ljt;
     *a.counter = 0ull;
+    if (a.flags[kFlagListTrunc])
+      a.flags[kFlagTruncEvals] += 1;
   }
 }
 
@@ -161,6 +164,7 @@ cudaError_t launch_finalize(mmnb_handle *h, double *d_f, double *d_energy)
   a.any_q = h->any_q ? 1 : 0;
   a.wsum = h->used_water ? h->d_wsum : nullptr;
   a.counter = h->d_wsum + 2;
+  a.flags = h->d_flags;
   a.tail = h->cfg.include_lj_correction ? h->lj_correction : 0.0;
   a.energy = d_energy;
   k_finalize<<<h->elec_blocks, kFinThreads, 0, h->stream>>>(a);

@@ -42,6 +42,7 @@ struct mmnb_md {
   int ke_blocks = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  long gen = -1;                // the handle's buffer generation at the capture
   std::string err;
 };
 
@@ -54,6 +55,7 @@ struct mmnb_md_batch {
   std::vector<cudaEvent_t> done;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  std::vector<long> gen;        // each replica handle's buffer generation at the capture
   std::string err;
 };
 
@@ -457,6 +459,7 @@ static int md_capture(mmnb_md *md, double *log)
   MDCK(ec);
   md->graph = g;
   MDCK(cudaGraphInstantiate(&md->exec, g, cudaGraphInstantiateFlagUseNodePriority));
+  md->gen = h->buf_gen;
   return MMNB_OK;
 }
 
@@ -484,7 +487,9 @@ int mmnb_md_run(mmnb_md *md, int nsteps, double *energies)
     return MMNB_OK;
   if (const int s = md_reserve_log(md, nsteps))
     return s;
-  if (!md->exec) {
+  // captured again when the handle's buffers were reallocated since (rows
+  // regrown, mmnb_scale, mmnb_set_params): the graph holds their addresses
+  if (!md->exec || md->gen != h->buf_gen) {
     const int s = md_capture(md, md->d_log);
     if (s)
       return s;
@@ -501,10 +506,13 @@ int mmnb_md_run(mmnb_md *md, int nsteps, double *energies)
   MDCK(cudaStreamSynchronize(h->stream));
   h->evals += nsteps;
   h->first = false;
-  if (flags[kFlagOverflow] > 0)
-    return md_fail(md, MMNB_ERR_OVERFLOW,
-                   "a neighbour row outgrew its capacity during the run (" + std::to_string(flags[kFlagOverflow]) +
-                       " entries); evaluate once with mmnb_compute to grow the rows, then run again");
+  (void) flags;
+  // rows cut at their capacity or a non-finite coordinate during the run: the
+  // status says which; after an overflow the rows are regrown, so running again
+  // from a saved state evaluates complete rows
+  long trunc = 0;
+  if (const int st = mmnb_check(h, &trunc, nullptr))
+    return md_fail(md, st, std::string("during the run: ") + h->err);
   return MMNB_OK;
 }
 
@@ -633,6 +641,9 @@ static int batch_capture(mmnb_md_batch *b)
   e = cudaGraphInstantiate(&b->exec, g, cudaGraphInstantiateFlagUseNodePriority);
   if (e != cudaSuccess)
     return batch_fail(b, MMNB_ERR_CUDA, cudaGetErrorString(e));
+  b->gen.clear();
+  for (mmnb_md *md : b->md)
+    b->gen.push_back(md->h->buf_gen);
   return MMNB_OK;
 }
 
@@ -651,9 +662,18 @@ int mmnb_md_batch_run(mmnb_md_batch *b, int nsteps, double *const *energies)
       b->exec = nullptr;
     }
   }
-  if (!b->exec)
+  // captured again when a replica handle's buffers were reallocated since
+  bool stale = !b->exec || b->gen.size() != b->md.size();
+  for (size_t i = 0; !stale && i < b->md.size(); i++)
+    stale = b->gen[i] != b->md[i]->h->buf_gen;
+  if (stale) {
+    if (b->exec) {
+      cudaGraphExecDestroy(b->exec);
+      b->exec = nullptr;
+    }
     if (const int s = batch_capture(b))
       return s;
+  }
   cudaError_t e = cudaSuccess;
   for (mmnb_md *md : b->md) {
     if (e == cudaSuccess)
@@ -683,8 +703,21 @@ int mmnb_md_batch_run(mmnb_md_batch *b, int nsteps, double *const *energies)
     md->h->evals += nsteps;
     overflow = std::max(overflow, flags[kFlagOverflow]);
   }
-  if (overflow > 0)
-    return batch_fail(b, MMNB_ERR_OVERFLOW, "a replica's neighbour row outgrew its capacity during the run");
+  (void) overflow;
+  // every replica's status (rows cut at capacity are regrown for the next run)
+  int status = MMNB_OK;
+  std::string msg;
+  for (size_t i = 0; i < b->md.size(); i++) {
+    long trunc = 0;
+    if (const int st = mmnb_check(b->md[i]->h, &trunc, nullptr)) {
+      if (!status) {
+        status = st;
+        msg = "replica " + std::to_string(i) + " during the run: " + b->md[i]->h->err;
+      }
+    }
+  }
+  if (status)
+    return batch_fail(b, status, msg);
   return MMNB_OK;
 }
 

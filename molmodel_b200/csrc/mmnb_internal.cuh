@@ -26,7 +26,10 @@ enum FlagIndex {
   // 4: evaluations, 5: rebuilds, 6: the list check's block counter
   kFlagPruneFull = 7,  // 1: the water kernel reads the full rows and writes the pruned ones
   kFlagPruneValid = 8, // 1 while the pruned rows belong to the current build
-  kFlagCount = 10
+  kFlagListTrunc = 9,  // 1 while the current list has rows cut at their capacity
+  kFlagTruncEvals = 10,// evaluations finished on such a list since the last mmnb_check
+  kFlagForceRebuild = 11, // 1: the next list check rebuilds (set by the host, cleared by the check)
+  kFlagCount = 12
 };
 
 // Box in the form the kernels use (cubic and orthorhombic).
@@ -159,6 +162,10 @@ struct mmnb_handle {
   double *d_plast = nullptr;
   double prune_margin = 0;           // 0: no pruning
   int *d_flags = nullptr;            // mmnb::kFlagCount ints
+  // bumped by every (re)allocation of a device buffer: a captured graph holds
+  // the addresses of its launch, so it is replayed only while this is unchanged
+  long buf_gen = 0;
+  long graph_gen = -1;               // buf_gen when mmnb_graph_capture ran
   int *h_flags = nullptr;            // pinned mirror
   long rebuilds = 0, evals = 0;
   long launches = 0;                 // kernels of this library launched so far

@@ -150,7 +150,8 @@ __global__ void __launch_bounds__(kCheckThreads) k_list_check(const double *__re
   __shared__ int rebuild_s;
   if (threadIdx.x == 0) {
     const int count = flags[4];
-    int rebuild = first || force || (__dadd_rn(b, a) > width);
+    int rebuild = first || force || flags[kFlagForceRebuild] || (__dadd_rn(b, a) > width);
+    flags[kFlagForceRebuild] = 0;
     if (interval > 0 && count % interval == 0)
       rebuild = 1;
     flags[kFlagRebuild] = rebuild;
@@ -159,8 +160,10 @@ __global__ void __launch_bounds__(kCheckThreads) k_list_check(const double *__re
       flags[5] += 1;  // rebuild counter
     flags[6] = 0;
     rebuild_s = rebuild;
-    if (rebuild)
+    if (rebuild) {
       flags[kFlagPruneValid] = 0;
+      flags[kFlagListTrunc] = 0;
+    }
     flags[kFlagPruneFull] = prune > 0 ? (rebuild || !flags[kFlagPruneValid] || pa + pb > prune) : 1;
   }
   __syncthreads();
@@ -204,6 +207,10 @@ __device__ __forceinline__ void cell_assign(const RebuildArgs &a, int g)
   int ijk[3];
   for (int d = 0; d < 3; d++) {
     const double x = a.anchor[3 * g + d];
+    // a non-finite anchor converts to cell 0 (float-to-int conversion gives 0
+    // for NaN and saturates): flagged, the host reports it
+    if (!isfinite(x))
+      a.flags[kFlagError] = MMNB_ERR_DEVICE;
     ijk[d] = (int) floor(__dadd_rn(__ddiv_rn(x, a.cg.lc[d]), 0.5));
     ijk[d] %= n;
     if (ijk[d] < 0)
@@ -434,8 +441,10 @@ __device__ __forceinline__ void build_row(const RebuildArgs &a, int p, int lane,
   }
   if (lane == 0) {
     a.nbr_count[p] = min(count, a.rowcap);
-    if (count > a.rowcap)
+    if (count > a.rowcap) {
       atomicMax(&a.flags[kFlagOverflow], count);
+      a.flags[kFlagListTrunc] = 1;
+    }
     atomicMax(&a.flags[kFlagMaxRow], count);
   }
 }

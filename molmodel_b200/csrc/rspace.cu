@@ -318,7 +318,7 @@ __global__ void k_sort_sites(const double *__restrict__ r, const double *__restr
                              const double *__restrict__ sig, const double *__restrict__ eps,
                              const double *__restrict__ rscreen, const int *__restrict__ mask,
                              const int *__restrict__ sorted, const int *__restrict__ group, int ngroup, int G,
-                             double4 *__restrict__ sr, double4 *__restrict__ sp)
+                             double4 *__restrict__ sr, double4 *__restrict__ sp, int *__restrict__ flags)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ngroup * G)
@@ -327,7 +327,10 @@ __global__ void k_sort_sites(const double *__restrict__ r, const double *__restr
   const int g = sorted[p];
   const int site = group[2 * g] + k;
   if (site < group[2 * g + 1]) {
-    sr[s] = make_double4(r[3 * site], r[3 * site + 1], r[3 * site + 2], q[site]);
+    const double x = r[3 * site], y = r[3 * site + 1], z = r[3 * site + 2];
+    if (!isfinite(x) || !isfinite(y) || !isfinite(z))
+      flags[kFlagError] = MMNB_ERR_DEVICE;
+    sr[s] = make_double4(x, y, z, q[site]);
     sp[s] = make_double4(sig[site], sqrt(eps[site]), rscreen[site], (double) mask[site]);
   } else {
     sr[s] = make_double4(0, 0, 0, 0);
@@ -480,7 +483,8 @@ cudaError_t launch_sort_sites(mmnb_handle *h, const double *d_r)
 {
   const int n = h->ngroup * h->G;
   k_sort_sites<<<div_up(n, 256), 256, 0, h->stream>>>(d_r, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_mask,
-                                                      h->d_sorted, h->d_group, h->ngroup, h->G, h->d_sr, h->d_sp);
+                                                      h->d_sorted, h->d_group, h->ngroup, h->G, h->d_sr, h->d_sp,
+                                                      h->d_flags);
   h->launches += 1;
   return cudaGetLastError();
 }

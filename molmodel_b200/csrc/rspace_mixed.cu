@@ -806,7 +806,8 @@ __global__ void k_prep_mixed(const double *__restrict__ r, const double *__restr
                              const double *__restrict__ rscreen, const int *__restrict__ mask,
                              const int *__restrict__ sorted, const int *__restrict__ group, int ngroup, int G,
                              int water, float4 *__restrict__ site, float4 *__restrict__ par,
-                             double4 *__restrict__ anchor, unsigned long long *__restrict__ wsum)
+                             double4 *__restrict__ anchor, unsigned long long *__restrict__ wsum,
+                             int *__restrict__ flags)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < 2)
@@ -821,6 +822,11 @@ __global__ void k_prep_mixed(const double *__restrict__ r, const double *__restr
   const double ax = r[3 * a0], ay = r[3 * a0 + 1], az = r[3 * a0 + 2];
   if (k == 0)
     anchor[p] = make_double4(ax, ay, az, 0.0);
+  // a non-finite coordinate is flagged (the host reports it); every index
+  // below stays in range whatever the coordinates
+  if (a0 + k < group[2 * g + 1] &&
+      !isfinite(r[3 * (a0 + k)] + r[3 * (a0 + k) + 1] + r[3 * (a0 + k) + 2]))
+    flags[kFlagError] = MMNB_ERR_DEVICE;
   if (water) {
     // G == 3: slot k of group p from the two H sites (a0 + 1, a0 + 2) and O
     const int h1 = a0 + 1, h2 = a0 + 2;
@@ -852,7 +858,7 @@ cudaError_t launch_prep_mixed(mmnb_handle *h, const double *d_r)
   const int water = h->water && !h->want_fields && h->cfg.include_rspace;
   k_prep_mixed<<<div_up(n, 256), 256, 0, h->stream>>>(d_r, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_mask,
                                                       h->d_sorted, h->d_group, h->ngroup, h->G, water, h->mx.site,
-                                                      h->mx.par, h->mx.anchor, h->d_wsum);
+                                                      h->mx.par, h->mx.anchor, h->d_wsum, h->d_flags);
   h->launches += 1;
   return cudaGetLastError();
 }

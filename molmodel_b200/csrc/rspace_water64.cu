@@ -299,12 +299,13 @@ __global__ void __launch_bounds__(kW64Warps * 32, MMNB_W64_BLOCKS) k_pair_water6
 
 // Per step: sorted FP64 anchors and the 96-byte records of the partner side,
 // (h1x, h1y, h1z, h2x), (h2y, h2z, qO, qH1), (qH2, sigma_O, sqrt(eps_O), 0) with
-// the H positions taken from the anchor O; the row counter is cleared.
+// the H positions taken from the anchor O; the row counter is cleared and a
+// non-finite coordinate is flagged.
 __global__ void k_sort_water64(const double *__restrict__ r, const double *__restrict__ q,
                                const double *__restrict__ sig, const double *__restrict__ eps,
                                const int *__restrict__ sorted, const int *__restrict__ group, int ngroup,
                                double4 *__restrict__ anchor, double4 *__restrict__ rec,
-                               unsigned long long *__restrict__ counter)
+                               unsigned long long *__restrict__ counter, int *__restrict__ flags)
 {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p == 0)
@@ -314,6 +315,8 @@ __global__ void k_sort_water64(const double *__restrict__ r, const double *__res
   const int a0 = group[2 * sorted[p]];
   const double ax = r[3 * a0], ay = r[3 * a0 + 1], az = r[3 * a0 + 2];
   const double *h1 = r + 3 * (a0 + 1), *h2 = r + 3 * (a0 + 2);
+  if (!isfinite(ax + ay + az + h1[0] + h1[1] + h1[2] + h2[0] + h2[1] + h2[2]))
+    flags[kFlagError] = MMNB_ERR_DEVICE;
   anchor[p] = make_double4(ax, ay, az, 0.0);
   rec[3 * (size_t) p] = make_double4(h1[0] - ax, h1[1] - ay, h1[2] - az, h2[0] - ax);
   rec[3 * (size_t) p + 1] = make_double4(h2[1] - ay, h2[2] - az, q[a0], q[a0 + 1]);
@@ -328,7 +331,8 @@ static size_t water64_smem(const mmnb_handle *h)
 cudaError_t launch_sort_water64(mmnb_handle *h, const double *d_r)
 {
   k_sort_water64<<<div_up(h->ngroup, 256), 256, 0, h->stream>>>(
-      d_r, h->d_q, h->d_sig, h->d_eps, h->d_sorted, h->d_group, h->ngroup, h->d_sp, h->d_sr, h->d_wsum + 3);
+      d_r, h->d_q, h->d_sig, h->d_eps, h->d_sorted, h->d_group, h->ngroup, h->d_sp, h->d_sr, h->d_wsum + 3,
+      h->d_flags);
   h->launches += 1;
   return cudaGetLastError();
 }

@@ -158,6 +158,16 @@ class ElecLJ:
         self.energy = dict(elec=e.elec, lj=e.lj, lj_correction=e.lj_correction, total=e.total)
         return uu.value
 
+    def check(self):
+        """mmnb_check: status of the evaluations since the last check on device
+        arrays.  Returns (truncated evaluations, longest row needed); raises
+        MmnbError (status MMNB_ERR_OVERFLOW or MMNB_ERR_DEVICE) when rows were
+        cut at their capacity or a coordinate was not finite."""
+        t = ctypes.c_long(0)
+        m = ctypes.c_int(0)
+        check(load().mmnb_check(self._h, ctypes.byref(t), ctypes.byref(m)), self._h)
+        return t.value, m.value
+
     def virial(self, r, masses, molecules=None):
         """dU/ds at s = 1 along the reference's volume-move path (mmnb_virial):
         box x s, each molecule moved rigidly so its centre of mass is x s,
