@@ -108,7 +108,7 @@ def esp_fixture(ref):
 
 
 def main():
-    reference_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    reference_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MMNB_REFERENCE", "/root/reference")
     ref = reference()
     if ref is None:
         raise SystemExit("oracle/_ref/libref.so is missing: run `make -C oracle ref` first")
