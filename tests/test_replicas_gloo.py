@@ -44,8 +44,7 @@ def _free_port():
     return p
 
 
-def test_ranks_agree_on_the_exchange():
-    world = 2
+def _run_ranks(world):
     port = _free_port()
     procs = []
     for r in range(world):
@@ -55,15 +54,27 @@ def test_ranks_agree_on_the_exchange():
     outs = []
     for p in procs:
         try:
-            so, se = p.communicate(timeout=180)
+            so, se = p.communicate(timeout=240)
         except subprocess.TimeoutExpired:
             for q in procs:
                 q.kill()
             raise
         assert p.returncode == 0, se
         outs.append(json.loads(so.strip().splitlines()[-1]))
-    a, b = outs
+    return outs
+
+
+def test_exchange_loop_over_two_ranks_matches_one_process():
+    """The full loop (advance, one all-gather of (id, T, U), the same Metropolis
+    pass on every rank, velocity rescaling of the swapped replicas) on two gloo
+    ranks gives the single process's temperature history and energies."""
+    a, b = _run_ranks(2)
+    (one,) = _run_ranks(1)
     assert sorted(a["mine"] + b["mine"]) == list(range(6))
-    assert a["energies"] == b["energies"] and a["temps"] == b["temps"] and a["accepted"] == b["accepted"]
-    sizes = [256, 4096, 1024, 512, 2048, 300]
-    assert dict(map(tuple, a["energies"])) == {rid: -10.0 * sizes[rid] - rid for rid in range(6)}
+    assert a["history"] == b["history"] == one["history"]
+    assert a["accepted"] == b["accepted"] == one["accepted"] and a["attempts"] == 4
+    assert a["energies"] == b["energies"] == one["energies"]
+    # temperatures move: some swap was accepted, and the ladder is kept
+    assert one["accepted"] > 0
+    for h in one["history"]:
+        assert sorted(t for _, t in h) == sorted(t for _, t in one["history"][0])
