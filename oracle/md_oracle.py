@@ -19,7 +19,9 @@ ConstraintGroup::constrain_velocities: one solve with the current derivatives.
 The water's three constraints are taken as the distances O-H1, O-H2 and H1-H2
 (the reference states the angle as an angle constraint; both describe the
 same rigid triangle and span the same constraint normals, so both converge
-to the same positions and velocities).
+to the same positions and velocities).  ReferenceConstraints runs the
+reference's own ConstraintGroup instead (oracle/_ref/libref.so), and
+tests/test_md_oracle.py checks that the two agree.
 """
 import numpy as np
 
@@ -73,16 +75,49 @@ def water_lengths(r_oh=1.0, angle_deg=109.47):
     return np.array([r_oh, r_oh, r_hh])
 
 
-def run(evaluate, r, v, masses, dt, steps, lengths):
+class RestatedConstraints:
+    """The constraint solves above (three distances per water)."""
+
+    def __init__(self, lengths):
+        self.lengths = lengths
+
+    def positions(self, x0, x, v, minv, dt):
+        constrain_positions(x0, x, v, minv, self.lengths, dt)
+
+    def velocities(self, x, v, minv):
+        constrain_velocities(x, v, minv)
+
+
+class ReferenceConstraints:
+    """The reference's own ConstraintGroup solves (oracle/_ref/libref.so:
+    src/constraint.cpp with the O-H lengths and the H-O-H angle), iterated
+    to tol in the reference's constraint units."""
+
+    def __init__(self, lib, r_oh=1.0, angle_deg=109.47, tol=1e-13):
+        self.lib, self.r_oh, self.angle, self.tol = lib, r_oh, angle_deg, tol
+
+    def positions(self, x0, x, v, minv, dt):
+        r, vv = self.lib.water_constrain_positions(x0, x, v, 1.0 / minv[0], dt, self.r_oh, self.angle, self.tol)
+        x[...] = r.reshape(x.shape)
+        v[...] = vv.reshape(v.shape)
+
+    def velocities(self, x, v, minv):
+        v[...] = self.lib.water_constrain_velocities(x, v, 1.0 / minv[0], self.r_oh, self.angle).reshape(v.shape)
+
+
+def run(evaluate, r, v, masses, dt, steps, lengths, constraints=None):
     """evaluate(r (nsite,3)) -> (forces (nsite,3), potential energy).
-    masses in the reference's mass unit.  Returns the final r, v and an array
-    (steps, 3) of kinetic, potential and conserved energy."""
+    masses in the reference's mass unit; constraints: the solver of the
+    position and velocity constraints (default: the restatement above).
+    Returns the final r, v and an array (steps, 3) of kinetic, potential and
+    conserved energy."""
     nmol = len(r) // 3
     x = np.array(r, dtype=np.float64).reshape(nmol, 3, 3)
     vv = np.array(v, dtype=np.float64).reshape(nmol, 3, 3)
     m = np.asarray(masses, dtype=np.float64).reshape(nmol, 3)
     minv = 1.0 / m
-    constrain_velocities(x, vv, minv)
+    cs = constraints or RestatedConstraints(lengths)
+    cs.velocities(x, vv, minv)
     f, u = evaluate(x.reshape(-1, 3))
     f = f.reshape(nmol, 3, 3)
     out = np.zeros((steps, 3))
@@ -90,11 +125,11 @@ def run(evaluate, r, v, masses, dt, steps, lengths):
         vv += 0.5 * dt * f * minv[..., None]
         x0 = x.copy()
         x += dt * vv
-        constrain_positions(x0, x, vv, minv, lengths, dt)
+        cs.positions(x0, x, vv, minv, dt)
         f, u = evaluate(x.reshape(-1, 3))
         f = f.reshape(nmol, 3, 3)
         vv += 0.5 * dt * f * minv[..., None]
-        constrain_velocities(x, vv, minv)
+        cs.velocities(x, vv, minv)
         ke = 0.5 * float((m[..., None] * vv * vv).sum())
         out[s] = (ke, u, ke + u)
     return x.reshape(-1, 3), vv.reshape(-1, 3), out

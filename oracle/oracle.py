@@ -133,6 +133,16 @@ class OracleLib:
         L.orc_eleclj_phi_at_points.argtypes = [_vp, _dp, ctypes.c_int, _dp, _dp]
         L.orc_eleclj_delete.argtypes = [_vp]
         L.orc_pairset_demo.argtypes = [ctypes.c_int, ctypes.c_int, _ip, _ip, _ip, _ip]
+        # the reference's constraint solver (oracle/ref_constraint.cpp; libref.so only)
+        self.has_constraints = hasattr(L, "orc_water_constrain_positions")
+        if self.has_constraints:
+            L.orc_add_search_path.argtypes = [ctypes.c_char_p]
+            L.orc_add_search_path(os.path.join(HERE, "shim").encode())
+            L.orc_water_constrain_positions.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_double,
+                                                        ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                        ctypes.c_int]
+            L.orc_water_constrain_velocities.argtypes = [ctypes.c_int, _dp, _dp, _dp, ctypes.c_double,
+                                                         ctypes.c_double]
 
     # --- component entry points -------------------------------------------
     def chebyshev(self, rc, eta):
@@ -162,6 +172,22 @@ class OracleLib:
         self.lib.orc_p3m_field(h, _d(r), _d(q), _d(phi), _d(evec))
         self.lib.orc_p3m_delete(h)
         return phi, evec, tuple(int(x) for x in ngrid), chi.value
+
+    def water_constrain_positions(self, r0, r, v, mass3, dt, r_oh=1.0, angle_deg=109.47, tol=1e-12,
+                                  maxit=10000):
+        """ConstraintGroup::constrain_positions (src/constraint.cpp:295-335) on every
+        rigid water (two O-H lengths and the H-O-H angle): returns new r, v."""
+        r0, r, v = _f64(r0), _f64(r).copy(), _f64(v).copy()
+        nmol = r.size // 9
+        self.lib.orc_water_constrain_positions(nmol, _d(r0), _d(r), _d(v), _d(_f64(mass3)), dt, r_oh, angle_deg,
+                                               tol, maxit)
+        return r, v
+
+    def water_constrain_velocities(self, r, v, mass3, r_oh=1.0, angle_deg=109.47):
+        """ConstraintGroup::constrain_velocities (src/constraint.cpp:336-358): returns new v."""
+        r, v = _f64(r), _f64(v).copy()
+        self.lib.orc_water_constrain_velocities(r.size // 9, _d(r), _d(v), _d(_f64(mass3)), r_oh, angle_deg)
+        return v
 
     def pairset(self, n, adds):
         """Rows and membership matrix of a PairBinary built from ``adds``."""

@@ -7,7 +7,7 @@ import pytest
 from molmodel_b200 import ElecLJ, maxwell_boltzmann, water_box
 from molmodel_b200.md import MDyn, nve_drift
 from oracle import md_oracle
-from oracle.oracle import make_config, port
+from oracle.oracle import make_config, port, reference
 
 pytestmark = pytest.mark.gpu
 
@@ -24,9 +24,17 @@ def _bond_errors(r, nmol):
     return np.abs(dist - md_oracle.water_lengths()[None, :]).max()
 
 
-def test_fp64_md_follows_the_reference_step():
+@pytest.mark.parametrize("solver", ["restated", "reference"])
+def test_fp64_md_follows_the_reference_step(solver):
     """216 waters, ordinary Ewald (kc 7), 1 fs, 10 steps: SETTLE + the 3x3
-    velocity solve against SHAKE/RATTLE iterated to 1e-12 A."""
+    velocity solve against the reference's step with its constraint solves
+    iterated to convergence -- restated (three distances), or the reference's
+    own ConstraintGroup (two O-H lengths and the H-O-H angle,
+    src/constraint.cpp:295-358) with the reference's own energies, where the
+    reference build is present."""
+    ref = reference()
+    if solver == "reference" and (ref is None or not ref.has_constraints):
+        pytest.skip("the reference build (oracle/_ref) is not present")
     wb = water_box(6, seed=1)
     cfg = _ksum_cfg()
     v0 = maxwell_boltzmann(wb, 300.0, seed=3)
@@ -37,15 +45,17 @@ def test_fp64_md_follows_the_reference_step():
     r_gpu, v_gpu = md.state()
     md.close()
 
-    o = port().eleclj(make_config(wb.box, **cfg), wb.nsite, wb.groups, wb.exclusions, wb.site_mask, wb.q,
-                      wb.sigma, wb.epsilon, wb.rscreen)
+    lib = ref if solver == "reference" else port()
+    o = lib.eleclj(make_config(wb.box, **cfg), wb.nsite, wb.groups, wb.exclusions, wb.site_mask, wb.q,
+                   wb.sigma, wb.epsilon, wb.rscreen)
 
     def evaluate(r):
         out = o.eval(r)
         return out["f"], out["total"]
 
+    cs = md_oracle.ReferenceConstraints(ref) if solver == "reference" else None
     r_o, v_o, e_o = md_oracle.run(evaluate, wb.positions, v0, wb.masses * MASS_UNIT, 0.001, 10,
-                                  md_oracle.water_lengths())
+                                  md_oracle.water_lengths(), constraints=cs)
     assert np.abs(r_gpu - r_o).max() < 1e-9
     assert np.abs(v_gpu - v_o).max() < 1e-6 * np.abs(v_o).max()
     assert np.abs(e_gpu - e_o).max() < 1e-8 * np.abs(e_o[:, 2]).max()

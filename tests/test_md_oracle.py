@@ -2,9 +2,14 @@
 constraint solves and the integrator on forces simple enough to check by
 hand.  The GPU integrator is compared with it in test_gpu_md.py."""
 import numpy as np
+import pytest
 
 from molmodel_b200 import maxwell_boltzmann, water_box
 from oracle import md_oracle
+from oracle.oracle import reference
+
+needs_reference = pytest.mark.skipif(reference() is None or not reference().has_constraints,
+                                     reason="the reference build (oracle/_ref) is not present")
 
 MASS_UNIT = 1.0 / 418.4
 
@@ -51,3 +56,39 @@ def test_free_rigid_waters_keep_their_kinetic_energy():
     _, _, e = md_oracle.run(lambda r: (np.zeros_like(r), 0.0), wb.positions, v, masses, 0.0005, 200,
                             md_oracle.water_lengths())
     assert np.abs(e[:, 0] / e[0, 0] - 1).max() < 1e-4
+
+
+@needs_reference
+def test_constraint_solves_match_the_reference_constraint_group():
+    """The restated solves (three distances) against the reference's own
+    ConstraintGroup (two O-H lengths and the H-O-H angle, src/constraint.cpp:
+    295-358): the same converged positions and velocities."""
+    wb, x0, m = _molecules(n=5, seed=3)
+    rng = np.random.default_rng(5)
+    v = rng.normal(size=x0.shape) * 8.0
+    x = x0 + 0.002 * v
+    xr, vr = x.copy(), v.copy()
+    md_oracle.constrain_positions(x0, xr, vr, 1 / m, md_oracle.water_lengths(), 0.002)
+    xf, vf = reference().water_constrain_positions(x0, x, v, m[0], 0.002, tol=1e-13)
+    assert np.abs(xf.reshape(x.shape) - xr).max() < 1e-11
+    assert np.abs(vf.reshape(v.shape) - vr).max() < 1e-11 / 0.002
+    w = rng.normal(size=x0.shape)
+    wr = w.copy()
+    md_oracle.constrain_velocities(xr, wr, 1 / m)
+    wf = reference().water_constrain_velocities(xr, w, m[0])
+    assert np.abs(wf.reshape(w.shape) - wr).max() < 1e-12
+
+
+@needs_reference
+def test_md_step_with_the_reference_constraints():
+    """200 steps of free rigid waters: the restated step with the reference's
+    constraint solver and with the restated one give the same trajectory."""
+    wb = water_box(3, seed=5)
+    v = maxwell_boltzmann(wb, 300.0, seed=7)
+    masses = wb.masses * MASS_UNIT
+    free = lambda r: (np.zeros_like(r), 0.0)
+    ra, va, ea = md_oracle.run(free, wb.positions, v, masses, 0.0005, 200, md_oracle.water_lengths())
+    rb, vb, eb = md_oracle.run(free, wb.positions, v, masses, 0.0005, 200, md_oracle.water_lengths(),
+                               constraints=md_oracle.ReferenceConstraints(reference()))
+    assert np.abs(ra - rb).max() < 1e-10
+    assert np.abs(ea - eb).max() < 1e-10 * np.abs(ea).max()
