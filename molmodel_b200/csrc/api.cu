@@ -429,7 +429,7 @@ void free_all(mmnb_handle *h)
     h->ev_flags = nullptr;
   }
   void *ptrs[] = {h->d_group, h->d_excl_ptr, h->d_excl_idx, h->d_p14_ptr, h->d_p14_idx, h->d_gexcl_ptr,
-                  h->d_gexcl_idx, h->d_mask, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_cheb, h->d_cheb_w, h->d_cheb_d, h->d_lj_row,
+                  h->d_gexcl_idx, h->d_mask, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_cheb, h->d_cheb_w, h->d_cheb_d, h->d_lj_row, h->d_lj_row_part,
                   h->d_vir_part, h->d_vir_row, h->d_vir_mol, h->d_vir_molw, h->d_vir_mass,
                   h->d_stencil, h->d_cell_rank, h->d_cell_of_rank, h->d_cell_of_group, h->d_cell_count,
                   h->d_cell_start, h->d_slot, h->d_sorted, h->d_rank, h->d_anchor, h->d_last, h->d_anchor_sorted, h->d_anchor32, h->d_block_sum,
@@ -723,7 +723,7 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
       (s = dalloc(h, &h->d_ljf, 3 * (size_t) nsite)) || (s = dalloc(h, &h->d_lj_part, nlj)) ||
       (s = dalloc(h, &h->d_lj_row, ngroup)) || (s = dalloc(h, &h->d_vir_part, nlj)) ||
       (s = dalloc(h, &h->d_vir_row, ngroup)) ||
-      (s = dalloc(h, &h->d_elec_part, h->elec_blocks)) || (s = dalloc(h, &h->d_energy, 8)) ||
+      (s = dalloc(h, &h->d_elec_part, h->elec_blocks)) || (s = dalloc(h, &h->d_lj_row_part, h->elec_blocks)) || (s = dalloc(h, &h->d_energy, 8)) ||
       (s = dalloc(h, &h->d_r, 3 * (size_t) nsite)) || (s = dalloc(h, &h->d_f, 3 * (size_t) nsite)) ||
       (s = dalloc(h, &h->d_wsum, 8)))
     return s;

@@ -26,6 +26,7 @@ struct FinArgs {
   int lj_lo, lj_hi, any_q;
   const double *lj_row;               // FP64 water kernel: per-row LJ energies [0, nrow), or null
   int nrow;
+  double *lj_row_part;                // per block: its slice of lj_row
   const unsigned long long *wsum;     // water kernel's fixed-point pair energies, or null
   unsigned long long *counter;        // finished-block counter, left at 0
   int *flags;                         // list flags: counts evaluations finished on cut rows
@@ -100,8 +101,19 @@ __global__ void __launch_bounds__(kFinThreads) k_finalize(FinArgs a)
     }
   }
   const double bs = block_sum(e, se);
+  double rs = 0;
+  if (a.lj_row) {
+    // this block's slice of the per-row LJ energies (fixed slices, fixed order)
+    const int per = (a.nrow + gridDim.x - 1) / gridDim.x;
+    const int lo = blockIdx.x * per, hi = min(a.nrow, lo + per);
+    for (int k = lo + threadIdx.x; k < hi; k += blockDim.x)
+      rs += a.lj_row[k];
+    rs = block_sum(rs, se);
+  }
   if (threadIdx.x == 0) {
     a.elec_part[blockIdx.x] = bs;
+    if (a.lj_row)
+      a.lj_row_part[blockIdx.x] = rs;
     __threadfence();
     last = atomicAdd(a.counter, 1ull) == gridDim.x - 1;
   }
@@ -115,8 +127,8 @@ __global__ void __launch_bounds__(kFinThreads) k_finalize(FinArgs a)
   for (int k = a.lj_lo + threadIdx.x; k < a.lj_hi; k += blockDim.x)
     lj += a.lj_part[k];
   if (a.lj_row)
-    for (int k = threadIdx.x; k < a.nrow; k += blockDim.x)
-      lj += a.lj_row[k];
+    for (int k = threadIdx.x; k < (int) gridDim.x; k += blockDim.x)
+      lj += a.lj_row_part[k];
   el = block_sum(el, se);
   lj = block_sum(lj, se);
   if (threadIdx.x == 0) {
@@ -160,6 +172,7 @@ cudaError_t launch_finalize(mmnb_handle *h, double *d_f, double *d_energy)
   a.lj_lo = (h->used_water || h->used_water64) ? h->lj_pair_blocks : 0;
   a.lj_row = h->used_water64 ? h->d_lj_row : nullptr;
   a.nrow = h->ngroup;
+  a.lj_row_part = h->d_lj_row_part;
   a.lj_hi = h->lj_pair_blocks + h->lj_excl_blocks;
   a.any_q = h->any_q ? 1 : 0;
   a.wsum = h->used_water ? h->d_wsum : nullptr;

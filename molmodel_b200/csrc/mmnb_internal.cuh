@@ -182,6 +182,7 @@ struct mmnb_handle {
   double *d_phi = nullptr, *d_evec = nullptr, *d_ljf = nullptr;
   double *d_lj_part = nullptr;       // LJ energy partials: pair-kernel blocks, then exclusion blocks
   double *d_lj_row = nullptr;        // FP64 water kernel: LJ energy of each row (sorted order)
+  double *d_lj_row_part = nullptr;   // finalize: per block, its slice of d_lj_row
   // mmnb_virial: the pair kernels' virial term (per block: pair-kernel blocks,
   // then exclusion blocks; per row: FP64 water kernel), molecule ranges,
   // masses and per-molecule sums (allocated on first use)
