@@ -274,18 +274,42 @@ int mmnb_get_tuning(mmnb_handle *h, int tuning[3]);
 int mmnb_set_tuning(mmnb_handle *h, const int tuning[3]);
 
 /* ---- adjoint --------------------------------------------------------------
-   Gradients of one evaluation with respect to uniform scales of all charges,
-   all LJ sigmas and all LJ epsilons (each at 1), for the force-field fits the
-   reference runs through WeakCouple::update and BCIFit (src/msimprog.cpp:855-876,
+   Per-site parameter gradients, for the force-field fits the reference runs
+   through WeakCouple::update and BCIFit (src/msimprog.cpp:855-876,
    src/bcifit.cpp:44-123) on the per-type parameters ElecLJ::types_changed maps
-   to sites (src/eleclj.cpp:440-503).  For rigid water with q_H = -q_O/2 and LJ
-   on O only, gradient / parameter value gives d/d(q_O, sigma_O, epsilon_O).
-   Runs the forward evaluation at r (f and u ADDED when non-NULL), then a
-   backward kernel that recomputes the LJ pair terms in FP64.
+   to sites (src/eleclj.cpp:440-503): a type's gradient is the sum of its
+   sites' gradients (times dq_site/dq_type where charges are tied).
+
+   mmnb_forward evaluates at r as mmnb_compute does with the site fields
+   requested (f and u ADDED when non-NULL, e when non-NULL) and keeps on the device what the gradients of this
+   evaluation need: the site potentials and fields.  It replaces the forward
+   pass of a fit; the backward does not evaluate again.
+
+   mmnb_site_gradients then returns, for that evaluation, per site i:
+     du_dq[i]   = dU/dq_i, the site potential (0 on sites without charge);
+     du_dsig[i] = dU/dsigma_i, du_deps[i] = dU/depsilon_i (0 on sites without
+                  LJ; LJ tail correction included, differentiated as a smooth
+                  function of the sites' sigma and epsilon);
+   and, given dl_df = dL/dF (3*nsite) of a loss of the forces the forward
+   returned, the same three for L:
+     dl_dq[i] = sum_k dl_df_k . dF_k/dq_i, dl_dsig[i], dl_deps[i].
+   dL/dq_i = g_i . E_i plus the potential at site i of the dipoles
+   p_j = q_j g_j (g = dl_df) and the switch and exclusion terms; the dipoles
+   need a second reciprocal-space solve (P3M mesh or Ewald sum), FP64 in both
+   precisions.  With the mixed form the gradients carry the forward's field
+   error (~1e-5 relative).  Any output may be NULL; with dl_df NULL the dl_*
+   outputs are left untouched.  MMNB_ERR_STATE unless the last evaluation of
+   the handle was mmnb_forward's (any other evaluation, mmnb_set_params or
+   mmnb_scale in between clears it). */
+int mmnb_forward(mmnb_handle *h, const double *r, double *f, double *u, mmnb_energy *e);
+int mmnb_site_gradients(mmnb_handle *h, const double *dl_df, double *du_dq, double *du_dsig, double *du_deps,
+                        double *dl_dq, double *dl_dsig, double *dl_deps);
+
+/* Gradients with respect to uniform scales of all charges, all LJ sigmas and
+   all LJ epsilons (each at 1): mmnb_forward at r, then mmnb_site_gradients
+   contracted with the site parameters, grad_u[k] = sum_i p_i dU/dp_i.
    grad_u[3]: dU/d(scales).  dl_df (3*nsite, may be NULL) is dL/dF of a loss of
-   the forces; grad_l[3] (may be NULL) receives sum_i dl_df_i . dF_i/d(scales).
-   MMNB_ERR_UNSUPPORTED unless every LJ site is its group's anchor and there
-   are no group exclusions or 1-4 pairs. */
+   the forces; grad_l[3] (may be NULL) receives sum_i dl_df_i . dF_i/d(scales). */
 int mmnb_backward(mmnb_handle *h, const double *r, const double *dl_df, double *f, double *u,
                   double grad_u[3], double grad_l[3]);
 

@@ -87,6 +87,8 @@ SIGNATURES = [
     ("mmnb_get_tuning", ctypes.c_int, [_vp, _ip]),
     ("mmnb_set_tuning", ctypes.c_int, [_vp, _ip]),
     ("mmnb_backward", ctypes.c_int, [_vp, _dp, _dp, _dp, _dp, _dp, _dp]),
+    ("mmnb_forward", ctypes.c_int, [_vp, _dp, _dp, _dp, ctypes.POINTER(MmnbEnergy)]),
+    ("mmnb_site_gradients", ctypes.c_int, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
     ("mmnb_phi_at_points", ctypes.c_int, [_vp, _dp, ctypes.c_int, _dp, _dp]),
     ("mmnb_virial", ctypes.c_int, [_vp, _dp, ctypes.c_int, _ip, _dp, _dp, _dp, ctypes.POINTER(MmnbEnergy), _dp]),
     ("mmnb_md_create", ctypes.c_int, [_vp, _dp, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,

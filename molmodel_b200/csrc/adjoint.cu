@@ -1,216 +1,568 @@
-// Adjoint of one evaluation with respect to three uniform parameter scales:
-// all charges (lambda_q), all LJ sigmas (lambda_s) and all LJ epsilons
-// (lambda_e), each at 1.  For rigid water with q_H = -q_O/2 and LJ on O only
-// these are the per-type parameters (q_O, sigma_O, epsilon_O) times their
-// values, the parameters WeakCouple and BCIFit update (src/msimprog.cpp:855-876,
-// src/bcifit.cpp:44-59, values mapped to sites by ElecLJ::types_changed,
+// Per-site parameter gradients of one evaluation (mmnb_forward, then
+// mmnb_site_gradients), for the force-field fits the reference runs on its
+// per-type parameters (WeakCouple::update, src/msimprog.cpp:855-876; BCIFit,
+// src/bcifit.cpp:44-123; types mapped to sites by ElecLJ::types_changed,
 // src/eleclj.cpp:440-503).
 //
-// Structure used (exact, no approximation):
-//   * every electrostatic term (real space with its switch-derivative share,
-//     reciprocal space, exclusions, self and neutralising terms) is a sum of
-//     q_i q_j products, so E_elec(lambda_q) = lambda_q^2 E_elec and likewise the
-//     electrostatic force: d/dlambda_q = 2 x (the electrostatic part);
-//   * the LJ pair energy with the group switch is S (A/r^12 - B/r^6) with
-//     A = 4 eps sig^12, B = 4 eps sig^6: linear in lambda_e, and its A and B
-//     parts scale as lambda_s^12 and lambda_s^6; the tail correction is linear
-//     in totA and totB (src/eleclj.cpp:294-308, 1247-1266).
-// The backward kernel recomputes the LJ pair terms of every listed group pair
-// inside the cutoff in FP64 (nothing from the forward pass is stored), splits
-// energy and force into their A and B parts, and contracts the forces with the
-// caller's dL/dF.  The electrostatic force is the forward force minus the LJ
-// force, so the charge gradient of the loss needs no second field solve.
+// Energy.  Every electrostatic term (switched real-space pairs, reciprocal
+// space, exclusion and 1-4 corrections, self and neutralising terms) is
+// q^T K q / 2 with K symmetric, and the forward's site potential is
+// phi = K q, so dU/dq_i = phi_i.  LJ pair energies are S(R) u(r) with
+// u = A/r^12 - B/r^6, A = 4 eps_ij sig_ij^12, B = 4 eps_ij sig_ij^6,
+// eps_ij = sqrt(eps_i eps_j), sig_ij = sqrt(sig_i sig_j) or (sig_i + sig_j)/2:
+// dA/dsig_i = 2 k A, dB/dsig_i = k B with k = 3/sig_i (geometric) or
+// 6/(sig_i + sig_j), and dA/deps_i = A/(2 eps_i), likewise B.
 //
-// Scope: LJ sites must be group anchors, without group exclusions or 1-4
-// pairs (rigid water and united-atom-like models); other systems return
-// MMNB_ERR_UNSUPPORTED.
+// Loss of the forces, g = dL/dF.  For a group pair (I, J) inside the cutoff
+// the forward puts q_a q_b S b1 d_ab on site a (d_ab = r_a - r_b with the
+// anchors' image shift, b1 = -(1/r) d/dr of the pair kernel) and the switch
+// force ds R T on the anchors (R the anchor displacement, T the summed
+// unswitched pair energies, ds = -2 dS/dR^2), opposite on J's side.  Hence
+//   dL/dq_i = g_i . E_i + sum_J [ -S sum_b q_b b1 (g_b . d_ib)
+//                                 + ds (g_A - g_B) . R sum_b q_b b0_ib ]
+//             + (the same dipole term for exclusion and 1-4 partners)
+//             + (the reciprocal-space potential of the dipoles q_j g_j),
+// with E_i the forward's field; and for LJ
+//   dL/dsig_i = sum_J sum_b [ S du'_ib (g_i - g_b) . d_ib + ds (g_A - g_B) . R u'_ib ]
+// where ' is d/dsig_i (d/deps_i alike).  The list is full (each group pair
+// in both rows), and every term above acts on the row's own sites, so one
+// warp per row writes its sites' sums with plain stores: no atomics, a fixed
+// summation order, the same rows and cutoff decisions as the forward.  The
+// reciprocal-space dipole solve is in pppm.cu / kspace.cu; the LJ tail
+// correction (linear in the class totals A and B) is added on the host.
 
+#include <cmath>
 #include <vector>
 
 #include "mmnb_internal.cuh"
 
 namespace mmnb {
 
-constexpr int kBwdWarps = 8;
+constexpr int kGradWarps = 4;
+constexpr int kGradThreads = 128;
 
-struct BwdArgs {
-  int ngroup, rowcap, geometric;
+// per-site output slots of the scratch area (each nsite doubles)
+enum GradSlot { kDuDq = 0, kDuDsig, kDuDeps, kDlDq, kDlDsig, kDlDeps, kGradSlots };
+
+struct GradArgs {
+  int nsite, ngroup, rowcap, geometric;
   Box box;
-  double rhi2, rlo2, inv_sw;
-  const double *r;        // positions (caller's order)
-  const double *dl_df;    // 3 * nsite, or null
-  const int *sorted, *group, *mask, *nbr, *nbr_count;
-  const double *sig, *eps;
-  double *partial;        // 4 per row: E_A, E_B, g.F_A, g.F_B
+  double rlo2, rhi2, inv_sw, eta;
+  double cheb_min, cheb_max, cheb_inv_dx;
+  const double *cheb;
+  const double *r, *q, *sig, *eps, *rscreen;
+  const double *g;  // dL/dF, 3 per site, or null
+  const int *mask, *nbr, *nbr_count, *sorted, *group;
+  const int *gexcl_ptr, *gexcl_idx, *excl_ptr, *excl_idx, *p14_ptr, *p14_idx;
+  double e14, l14;
+  int scale_e14, scale_l14, do14;
+  double *out;      // kGradSlots x nsite
 };
 
-// one warp per row group; lanes walk the row's list entries
-__global__ void __launch_bounds__(kBwdWarps * 32) k_lj_backward(BwdArgs a)
+// LJ pair energy u, force scalar du (force = du d), and their sigma_i
+// derivatives us, dus (eps_i derivatives: u / (2 eps_i), du / (2 eps_i))
+struct LJd {
+  double u, du, us, dus;
+};
+
+__device__ __forceinline__ LJd lj_terms(double si, double sj, double ei, double ej, int geometric, double r2)
+{
+  double sg, kap;
+  if (geometric) {
+    sg = si * sj;
+    kap = 3 / si;
+  } else {
+    const double hs = 0.5 * (si + sj);
+    sg = hs * hs;
+    kap = 6 / (si + sj);
+  }
+  const double s6 = sg * sg * sg;
+  const double b = 4 * sqrt(ei * ej) * s6, aa = b * s6;
+  const double ir2 = 1.0 / r2, ir6 = ir2 * ir2 * ir2;
+  const double a12 = aa * ir6 * ir6, b6 = b * ir6;
+  LJd t;
+  t.u = a12 - b6;
+  t.du = (12 * a12 - 6 * b6) * ir2;
+  t.us = kap * (2 * a12 - b6);
+  t.dus = kap * (24 * a12 - 6 * b6) * ir2;
+  return t;
+}
+
+__device__ __forceinline__ double3 load3(const double *p, int i)
+{
+  return make_double3(p[3 * i], p[3 * i + 1], p[3 * i + 2]);
+}
+
+// one warp per row (sorted group p); lanes walk the row's partners
+template <int G, bool SCREEN, bool GEXCL>
+__global__ void __launch_bounds__(kGradWarps * 32) k_grad_pair(GradArgs a)
 {
   const int lane = threadIdx.x & 31;
-  const int p = blockIdx.x * kBwdWarps + (threadIdx.x >> 5);
+  const int p = blockIdx.x * kGradWarps + (threadIdx.x >> 5);
   if (p >= a.ngroup)
-    return;
-  const int ai = a.group[2 * a.sorted[p]];
-  double ea = 0, eb = 0, ga = 0, gb = 0;
-  if (a.mask[ai] & MMNB_SITE_HAS_LJ) {
-    const double4 ri = make_double4(a.r[3 * ai], a.r[3 * ai + 1], a.r[3 * ai + 2], 0);
-    double gx = 0, gy = 0, gz = 0;
-    if (a.dl_df) {
-      gx = a.dl_df[3 * ai];
-      gy = a.dl_df[3 * ai + 1];
-      gz = a.dl_df[3 * ai + 2];
+    return;  // the whole warp
+  const int gi = a.sorted[p];
+  const int si0 = a.group[2 * gi], ns = a.group[2 * gi + 1] - si0;
+  double4 ri[G];
+  double3 gv[G];
+  double sgi[G], epi[G], rsi[G];
+  int mi[G];
+  double psi[G], dus[G], due[G], dls[G], dle[G];
+#pragma unroll
+  for (int k = 0; k < G; k++) {
+    psi[k] = dus[k] = due[k] = dls[k] = dle[k] = 0;
+    mi[k] = 0;
+    ri[k] = make_double4(0, 0, 0, 0);
+    gv[k] = make_double3(0, 0, 0);
+    sgi[k] = epi[k] = rsi[k] = 0;
+    if (k < ns) {
+      const int s = si0 + k;
+      ri[k] = make_double4(a.r[3 * s], a.r[3 * s + 1], a.r[3 * s + 2], a.q[s]);
+      if (a.g)
+        gv[k] = load3(a.g, s);
+      sgi[k] = a.sig[s];
+      epi[k] = a.eps[s];
+      rsi[k] = a.rscreen[s];
+      mi[k] = a.mask[s];
     }
-    const double si = a.sig[ai], ei = a.eps[ai];
-    const int cnt = a.nbr_count[p];
-    const int *row = a.nbr + (size_t) p * a.rowcap;
-    for (int e = lane; e < cnt; e += 32) {
-      const int aj = a.group[2 * a.sorted[row[e]]];
-      if (!(a.mask[aj] & MMNB_SITE_HAS_LJ))
-        continue;
-      const double4 rj = make_double4(a.r[3 * aj], a.r[3 * aj + 1], a.r[3 * aj + 2], 0);
-      double x, y, z, sx, sy, sz;
-      const double r2 = anchor_disp(a.box, ri, rj, x, y, z, sx, sy, sz);
-      if (r2 > a.rhi2)
-        continue;
-      double s = 1, ds = 0;
-      if (r2 > a.rlo2) {
-        const double zz = (r2 - a.rlo2) * a.inv_sw;
-        s = 1 + zz * zz * zz * (-10 + zz * (15 - 6 * zz));
-        ds = ((60 * zz - 120) * zz + 60) * zz * zz * a.inv_sw;
+  }
+  const int cnt = a.nbr_count[p];
+  const int *row = a.nbr + (size_t) p * a.rowcap;
+  for (int e = lane; e < cnt; e += 32) {
+    const int gj = a.sorted[row[e]];
+    const int sj0 = a.group[2 * gj], nsj = a.group[2 * gj + 1] - sj0;
+    const double4 rjA = make_double4(a.r[3 * sj0], a.r[3 * sj0 + 1], a.r[3 * sj0 + 2], 0);
+    double x, y, z, sx, sy, sz;
+    const double r2a = anchor_disp(a.box, ri[0], rjA, x, y, z, sx, sy, sz);
+    if (r2a > a.rhi2)
+      continue;
+    double S = 1, ds = 0;
+    if (r2a > a.rlo2) {
+      const double zz = (r2a - a.rlo2) * a.inv_sw;
+      S = ((-6 * zz + 15) * zz - 10) * zz * zz * zz + 1;
+      ds = ((60 * zz - 120) * zz + 60) * zz * zz * a.inv_sw;
+    }
+    double GR = 0;
+    if (a.g && ds != 0) {
+      const double3 gB = load3(a.g, sj0);
+      GR = (gv[0].x - gB.x) * x + (gv[0].y - gB.y) * y + (gv[0].z - gB.z) * z;
+    }
+    bool gx = false;
+    if (GEXCL)
+      gx = csr_has(a.gexcl_ptr, a.gexcl_idx, gi, gj);
+#pragma unroll
+    for (int jb = 0; jb < G; jb++) {
+      if (jb >= nsj)
+        break;
+      const int sj = sj0 + jb;
+      const int mj = a.mask[sj];
+      const double xj = a.r[3 * sj], yj = a.r[3 * sj + 1], zj = a.r[3 * sj + 2];
+      const double qj = a.q[sj];
+      const double3 gj3 = a.g ? load3(a.g, sj) : make_double3(0, 0, 0);
+#pragma unroll
+      for (int ia = 0; ia < G; ia++) {
+        const int m = mi[ia] & mj;
+        if (!m)
+          continue;
+        if (GEXCL && gx && csr_has(a.excl_ptr, a.excl_idx, si0 + ia, sj))
+          continue;
+        double dx, dy, dz, r2;
+        if (ia == 0 && jb == 0) {
+          dx = x;
+          dy = y;
+          dz = z;
+          r2 = r2a;
+        } else {
+          dx = (ri[ia].x + sx) - xj;
+          dy = (ri[ia].y + sy) - yj;
+          dz = (ri[ia].z + sz) - zj;
+          r2 = dx * dx + dy * dy + dz * dz;
+        }
+        if (m & MMNB_SITE_HAS_Q) {
+          double b0, b1, fseg;
+          int seg;
+          ewald_table_b(a.cheb, a.cheb_min, a.cheb_max, a.cheb_inv_dx, a.eta, r2, b0, b1, seg, fseg);
+          if (SCREEN) {
+            const double rs = rsi[ia] + a.rscreen[sj];
+            if (r2 < rs * rs) {
+              const double invr = 1.0 / sqrt(r2);
+              const double inv3 = 1.0 / (rs * rs * rs);
+              b0 += (-0.5 * r2 * inv3 + 1.5 / rs) - invr;
+              b1 += inv3 - invr * invr * invr;
+            }
+          }
+          const double gjd = gj3.x * dx + gj3.y * dy + gj3.z * dz;
+          psi[ia] += qj * (ds * GR * b0 - S * b1 * gjd);
+        }
+        if (m & MMNB_SITE_HAS_LJ) {
+          const LJd t = lj_terms(sgi[ia], a.sig[sj], epi[ia], a.eps[sj], a.geometric, r2);
+          const double gd = (gv[ia].x - gj3.x) * dx + (gv[ia].y - gj3.y) * dy + (gv[ia].z - gj3.z) * dz;
+          dus[ia] += S * t.us;
+          due[ia] += S * t.u;
+          dls[ia] += S * t.dus * gd + ds * GR * t.us;
+          dle[ia] += S * t.du * gd + ds * GR * t.u;
+        }
       }
-      const double sj = a.sig[aj], ej = a.eps[aj];
-      const double sg = a.geometric ? sqrt(si * sj) : 0.5 * (si + sj);
-      const double s6 = sg * sg * sg * sg * sg * sg;
-      const double b = 4 * sqrt(ei * ej) * s6;
-      const double ir2 = 1 / r2, ir6 = ir2 * ir2 * ir2;
-      const double bi6 = b * ir6, ai12 = b * s6 * ir6 * ir6;
-      ea += 0.5 * s * ai12;
-      eb += 0.5 * s * bi6;
-      // force on the row's anchor from each part, switch derivative included:
-      // -grad(S u) = (S du/dr2 * (-2) + u * ds) d
-      const double fa = 12 * ai12 * ir2 * s + ds * ai12;
-      const double fb = 6 * bi6 * ir2 * s + ds * bi6;
-      const double gd = gx * x + gy * y + gz * z;
-      ga += fa * gd;
-      gb += fb * gd;
     }
   }
 #pragma unroll
-  for (int o = 16; o; o >>= 1) {
-    ea += __shfl_xor_sync(0xffffffffu, ea, o);
-    eb += __shfl_xor_sync(0xffffffffu, eb, o);
-    ga += __shfl_xor_sync(0xffffffffu, ga, o);
-    gb += __shfl_xor_sync(0xffffffffu, gb, o);
+  for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+    for (int k = 0; k < G; k++) {
+      psi[k] += __shfl_xor_sync(0xffffffffu, psi[k], off);
+      dus[k] += __shfl_xor_sync(0xffffffffu, dus[k], off);
+      due[k] += __shfl_xor_sync(0xffffffffu, due[k], off);
+      dls[k] += __shfl_xor_sync(0xffffffffu, dls[k], off);
+      dle[k] += __shfl_xor_sync(0xffffffffu, dle[k], off);
+    }
   }
-  if (lane == 0) {
-    double *o = a.partial + 4 * (size_t) p;
-    o[0] = ea;
-    o[1] = eb;
-    o[2] = ga;
-    o[3] = gb;
+  const size_t n = a.nsite;
+#pragma unroll
+  for (int k = 0; k < G; k++) {
+    if (lane == k && k < ns) {
+      const int s = si0 + k;
+      a.out[kDlDq * n + s] += psi[k];
+      a.out[kDuDsig * n + s] += dus[k];
+      a.out[kDuDeps * n + s] += due[k];
+      a.out[kDlDsig * n + s] += dls[k];
+      a.out[kDlDeps * n + s] += dle[k];
+    }
   }
+}
+
+// exclusion corrections and 1-4 pairs, one thread per site over its own
+// partners (the forward's k_exclusions_fp64 terms)
+__global__ void __launch_bounds__(kGradThreads) k_grad_excl(GradArgs a)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nsite)
+    return;
+  const int mi = a.mask[i];
+  const double xi = a.r[3 * i], yi = a.r[3 * i + 1], zi = a.r[3 * i + 2];
+  const double3 gi = a.g ? load3(a.g, i) : make_double3(0, 0, 0);
+  double psi = 0, dus = 0, due = 0, dls = 0, dle = 0;
+  if ((mi & MMNB_SITE_HAS_Q) && a.g) {
+    for (int n = a.excl_ptr[i]; n < a.excl_ptr[i + 1]; n++) {
+      const int j = a.excl_idx[n];
+      if (!(a.mask[j] & MMNB_SITE_HAS_Q))
+        continue;
+      double x = xi - a.r[3 * j], y = yi - a.r[3 * j + 1], z = zi - a.r[3 * j + 2];
+      min_image_ref(a.box, x, y, z);
+      const double r2 = x * x + y * y + z * z;
+      const double rm = sqrt(r2);
+      const double er = a.eta * rm;
+      const double b0 = -erf(er) / rm;
+      const double b1 = (b0 + a.eta * M_2_SQRTPI * exp(-(er * er))) / r2;
+      const double3 gj = load3(a.g, j);
+      psi -= a.q[j] * b1 * (gj.x * x + gj.y * y + gj.z * z);
+    }
+  }
+  if (a.do14) {
+    for (int n = a.p14_ptr[i]; n < a.p14_ptr[i + 1]; n++) {
+      const int j = a.p14_idx[n];
+      const int m = mi & a.mask[j];
+      double x = xi - a.r[3 * j], y = yi - a.r[3 * j + 1], z = zi - a.r[3 * j + 2];
+      min_image_ref(a.box, x, y, z);
+      const double r2 = x * x + y * y + z * z;
+      const double3 gj = a.g ? load3(a.g, j) : make_double3(0, 0, 0);
+      if ((m & MMNB_SITE_HAS_Q) && a.g) {
+        const double rs = a.rscreen[i] + a.rscreen[j];
+        double b1;
+        if (r2 < rs * rs) {
+          b1 = 1.0 / (rs * rs * rs);
+        } else {
+          const double invr = 1.0 / sqrt(r2);
+          b1 = invr * invr * invr;
+        }
+        if (a.scale_e14)
+          b1 *= a.e14;
+        psi -= a.q[j] * b1 * (gj.x * x + gj.y * y + gj.z * z);
+      }
+      if (m & MMNB_SITE_HAS_LJ) {
+        const LJd t = lj_terms(a.sig[i], a.sig[j], a.eps[i], a.eps[j], a.geometric, r2);
+        const double l = a.scale_l14 ? a.l14 : 1.0;
+        const double gd = (gi.x - gj.x) * x + (gi.y - gj.y) * y + (gi.z - gj.z) * z;
+        dus += l * t.us;
+        due += l * t.u;
+        dls += l * t.dus * gd;
+        dle += l * t.du * gd;
+      }
+    }
+  }
+  const size_t n = a.nsite;
+  a.out[kDlDq * n + i] += psi;
+  a.out[kDuDsig * n + i] += dus;
+  a.out[kDuDeps * n + i] += due;
+  a.out[kDlDsig * n + i] += dls;
+  a.out[kDlDeps * n + i] += dle;
+}
+
+// dU/dq_i = phi_i; dL/dq_i += g_i . E_i; epsilon sums / (2 eps_i); zero on
+// sites without the parameter
+__global__ void k_grad_finish(int nsite, const int *__restrict__ mask, const double *__restrict__ eps,
+                              const double *__restrict__ g, const double *__restrict__ phi,
+                              const double *__restrict__ evec, double *__restrict__ out)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nsite)
+    return;
+  const size_t n = nsite;
+  const int m = mask[i];
+  if (m & MMNB_SITE_HAS_Q) {
+    out[kDuDq * n + i] = phi[i];
+    if (g)
+      out[kDlDq * n + i] += g[3 * i] * evec[3 * i] + g[3 * i + 1] * evec[3 * i + 1] + g[3 * i + 2] * evec[3 * i + 2];
+  } else {
+    out[kDuDq * n + i] = 0;
+    out[kDlDq * n + i] = 0;
+  }
+  if ((m & MMNB_SITE_HAS_LJ) && eps[i] > 0) {
+    const double inv = 0.5 / eps[i];
+    out[kDuDeps * n + i] *= inv;
+    out[kDlDeps * n + i] *= inv;
+  } else {
+    out[kDuDsig * n + i] = 0;
+    out[kDuDeps * n + i] = 0;
+    out[kDlDsig * n + i] = 0;
+    out[kDlDeps * n + i] = 0;
+  }
+}
+
+template <int G>
+static void launch_grad_pair_g(mmnb_handle *h, const GradArgs &a)
+{
+  const int blocks = div_up(h->ngroup, kGradWarps);
+  if (h->has_rscreen) {
+    if (h->any_gexcl)
+      k_grad_pair<G, true, true><<<blocks, kGradWarps * 32, 0, h->stream>>>(a);
+    else
+      k_grad_pair<G, true, false><<<blocks, kGradWarps * 32, 0, h->stream>>>(a);
+  } else {
+    if (h->any_gexcl)
+      k_grad_pair<G, false, true><<<blocks, kGradWarps * 32, 0, h->stream>>>(a);
+    else
+      k_grad_pair<G, false, false><<<blocks, kGradWarps * 32, 0, h->stream>>>(a);
+  }
+  h->launches += 1;
+}
+
+// FP64 meshes and plans of the dipole solve: the FP64 form's own (the forward
+// has finished with them), or, for the mixed form, a set made on first use
+static int grad_p3m_scratch(mmnb_handle *h, P3mScratch &s)
+{
+  const size_t nr = (size_t) h->mesh[0] * h->mesh[1] * h->mesh[2];
+  const size_t nk = (size_t) h->mesh[0] * h->mesh[1] * (h->mesh[2] / 2 + 1);
+  if (h->plan_r2c) {
+    s.r2c = h->plan_r2c;
+    s.c2r = h->plan_c2r;
+    if (h->cfg.p3m_ik_differentiate) {
+      s.spread = h->d_egrid;
+      s.spreadk = h->d_egridk;
+      s.solvek = h->d_meshk;
+      s.solve = h->d_mesh;
+    } else {
+      s.spread = s.solve = h->d_mesh;
+      s.spreadk = h->d_meshk;
+    }
+    return MMNB_OK;
+  }
+  if (h->cfg.p3m_ik_differentiate) {
+    h->err = "ik differentiation in the mixed form";
+    return MMNB_ERR_UNSUPPORTED;
+  }
+  if (!h->gplan_r2c) {
+    cudaError_t e = cudaMalloc(&h->d_gmesh, sizeof(double) * nr);
+    if (e == cudaSuccess)
+      e = cudaMalloc(&h->d_gmeshk, sizeof(cufftDoubleComplex) * nk);
+    if (e != cudaSuccess) {
+      h->err = std::string("gradient mesh: ") + cudaGetErrorString(e);
+      return MMNB_ERR_CUDA;
+    }
+    if (cufftPlan3d(&h->gplan_r2c, h->mesh[0], h->mesh[1], h->mesh[2], CUFFT_D2Z) != CUFFT_SUCCESS ||
+        cufftPlan3d(&h->gplan_c2r, h->mesh[0], h->mesh[1], h->mesh[2], CUFFT_Z2D) != CUFFT_SUCCESS) {
+      h->err = "gradient mesh: cuFFT plan";
+      return MMNB_ERR_CUDA;
+    }
+  }
+  s.r2c = h->gplan_r2c;
+  s.c2r = h->gplan_c2r;
+  s.spread = s.solve = h->d_gmesh;
+  s.spreadk = h->d_gmeshk;
+  return MMNB_OK;
 }
 
 }  // namespace mmnb
 
 using namespace mmnb;
 
-static int bwd_fail(mmnb_handle *h, int code, const std::string &msg)
+static int grad_fail(mmnb_handle *h, int code, const std::string &msg)
 {
   if (h)
     h->err = msg;
   return code;
 }
 
-extern "C" int mmnb_backward(mmnb_handle *h, const double *r, const double *dl_df, double *f, double *u,
-                             double grad_u[3], double grad_l[3])
+extern "C" int mmnb_site_gradients(mmnb_handle *h, const double *dl_df, double *du_dq, double *du_dsig,
+                                   double *du_deps, double *dl_dq, double *dl_dsig, double *dl_deps)
 {
-  if (!h || !r || !grad_u)
-    return bwd_fail(h, MMNB_ERR_ARG, "null handle, positions or gradient output");
-  if (!h->params_set)
-    return bwd_fail(h, MMNB_ERR_STATE, "mmnb_set_params has not been called");
-  if (!h->lj_on_anchors_only || h->any_gexcl || h->use_14)
-    return bwd_fail(h, MMNB_ERR_UNSUPPORTED,
-                "the backward pass covers LJ sites that are group anchors, without group exclusions or 1-4 pairs");
-  const size_t n3 = 3 * (size_t) h->nsite;
-  // forward pass (also brings the neighbour list up to date for r)
-  std::vector<double> fw(n3, 0.0);
-  mmnb_energy en;
-  int s = mmnb_compute(h, r, fw.data(), nullptr, &en, nullptr, nullptr);
-  if (s)
-    return s;
-  double gF = 0;
-  if (dl_df)
-    for (size_t k = 0; k < n3; k++)
-      gF += dl_df[k] * fw[k];
-  // LJ pair terms in FP64 over the current list; scratch kept by the handle
-  const size_t np = 4 * (size_t) h->ngroup;
-  if (h->bwd_cap < np + n3) {
+  if (!h)
+    return grad_fail(h, MMNB_ERR_ARG, "null handle");
+  if (!h->grad_ready)
+    return grad_fail(h, MMNB_ERR_STATE,
+                     "no evaluation to differentiate: call mmnb_forward first (any other evaluation, "
+                     "mmnb_set_params or mmnb_scale since then discards it)");
+  const size_t n = h->nsite, n3 = 3 * n;
+  const size_t nskd = h->kspace ? 2 * (size_t) h->nk : 0;
+  const size_t need = kGradSlots * n + n3 + nskd;
+  if (h->bwd_cap < need) {
     if (h->d_bwd)
       cudaFree(h->d_bwd);
     h->d_bwd = nullptr;
     h->bwd_cap = 0;
-    const cudaError_t ea = cudaMalloc(&h->d_bwd, (np + n3) * sizeof(double));
+    const cudaError_t ea = cudaMalloc(&h->d_bwd, need * sizeof(double));
     if (ea != cudaSuccess)
-      return bwd_fail(h, MMNB_ERR_CUDA, std::string("backward scratch: ") + cudaGetErrorString(ea));
-    h->bwd_cap = np + n3;
+      return grad_fail(h, MMNB_ERR_CUDA, std::string("gradient scratch: ") + cudaGetErrorString(ea));
+    h->bwd_cap = need;
   }
-  double *d_part = h->d_bwd, *d_g = dl_df ? h->d_bwd + np : nullptr;
-  std::vector<double> part(np);
-  BwdArgs a;
+  double *d_out = h->d_bwd, *d_g = dl_df ? h->d_bwd + kGradSlots * n : nullptr;
+  double *d_skd = h->d_bwd + kGradSlots * n + n3;
+  P3mScratch ps;
+  const bool p3m = h->any_q && h->cfg.include_kspace && h->p3m && dl_df;
+  if (p3m) {
+    const int st = grad_p3m_scratch(h, ps);
+    if (st)
+      return st;
+  }
+  GradArgs a;
+  a.nsite = h->nsite;
   a.ngroup = h->ngroup;
   a.rowcap = h->rowcap;
   a.geometric = h->cfg.geometric_combining_for_sigma;
   a.box = h->box;
-  a.rhi2 = h->rhi2;
   a.rlo2 = h->rlo2;
+  a.rhi2 = h->rhi2;
   a.inv_sw = h->inv_sw;
-  a.r = h->d_r;  // mmnb_compute left this evaluation's positions here
-  a.dl_df = d_g;
-  a.sorted = h->d_sorted;
-  a.group = h->d_group;
+  a.eta = h->eta;
+  a.cheb_min = h->cheb_min;
+  a.cheb_max = h->cheb_max;
+  a.cheb_inv_dx = h->cheb_inv_dx;
+  a.cheb = h->d_cheb;
+  a.r = h->d_r;  // the forward's positions (host path)
+  a.q = h->d_q;
+  a.sig = h->d_sig;
+  a.eps = h->d_eps;
+  a.rscreen = h->d_rscreen;
+  a.g = d_g;
   a.mask = h->d_mask;
   a.nbr = h->d_nbr;
   a.nbr_count = h->d_nbr_count;
-  a.sig = h->d_sig;
-  a.eps = h->d_eps;
-  a.partial = d_part;
-  cudaError_t e = cudaSuccess;
-  if (d_g)
+  a.sorted = h->d_sorted;
+  a.group = h->d_group;
+  a.gexcl_ptr = h->d_gexcl_ptr;
+  a.gexcl_idx = h->d_gexcl_idx;
+  a.excl_ptr = h->d_excl_ptr;
+  a.excl_idx = h->d_excl_idx;
+  a.p14_ptr = h->d_p14_ptr;
+  a.p14_idx = h->d_p14_idx;
+  // the forward's 1-4 terms: (factor - 1) x the full pair when scaling, the
+  // full pair otherwise (interact() as src/rspace.c:522-557 calls it)
+  a.e14 = h->cfg.elec_1_4_scale_factor - 1;
+  a.l14 = h->cfg.lj_1_4_scale_factor - 1;
+  a.scale_e14 = fabs(h->cfg.elec_1_4_scale_factor - 1) > 1e-10;
+  a.scale_l14 = fabs(h->cfg.lj_1_4_scale_factor - 1) > 1e-10;
+  a.do14 = h->use_14 ? 1 : 0;
+  a.out = d_out;
+  cudaError_t e = cudaMemsetAsync(d_out, 0, sizeof(double) * kGradSlots * n, h->stream);
+  if (e == cudaSuccess && d_g)
     e = cudaMemcpyAsync(d_g, dl_df, n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
-  if (e == cudaSuccess) {
-    k_lj_backward<<<div_up(h->ngroup, kBwdWarps), kBwdWarps * 32, 0, h->stream>>>(a);
+  if (e == cudaSuccess && h->cfg.include_rspace) {
+    switch (h->G) {
+    case 1: launch_grad_pair_g<1>(h, a); break;
+    case 2: launch_grad_pair_g<2>(h, a); break;
+    case 3: launch_grad_pair_g<3>(h, a); break;
+    case 4: launch_grad_pair_g<4>(h, a); break;
+    default: launch_grad_pair_g<8>(h, a); break;
+    }
+    k_grad_excl<<<div_up(h->nsite, kGradThreads), kGradThreads, 0, h->stream>>>(a);
+    h->launches += 1;
     e = cudaGetLastError();
   }
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(part.data(), d_part, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess && d_g && h->any_q && h->cfg.include_kspace) {
+    if (h->p3m)
+      e = launch_p3m_dipole_fp64(h, h->d_r, d_g, ps, d_out + kDlDq * n);
+    else if (h->kspace)
+      e = launch_kspace_dipole(h, h->d_r, d_g, d_skd, d_out + kDlDq * n);
+  }
+  if (e == cudaSuccess) {
+    k_grad_finish<<<div_up(h->nsite, kGradThreads), kGradThreads, 0, h->stream>>>(h->nsite, h->d_mask, h->d_eps,
+                                                                                   d_g, h->d_phi, h->d_evec, d_out);
+    h->launches += 1;
+    e = cudaGetLastError();
+  }
+  double *outs[kGradSlots] = {du_dq, du_dsig, du_deps, dl_df ? dl_dq : nullptr, dl_df ? dl_dsig : nullptr,
+                              dl_df ? dl_deps : nullptr};
+  for (int k = 0; k < kGradSlots && e == cudaSuccess; k++)
+    if (outs[k])
+      e = cudaMemcpyAsync(outs[k], d_out + k * n, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess)
     e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess)
-    return bwd_fail(h, MMNB_ERR_CUDA, std::string("backward pass: ") + cudaGetErrorString(e));
-  // fixed-order sums
-  double ea = 0, eb = 0, ga = 0, gb = 0;
-  for (int p = 0; p < h->ngroup; p++) {
-    ea += part[4 * p];
-    eb += part[4 * p + 1];
-    ga += part[4 * p + 2];
-    gb += part[4 * p + 3];
+    return grad_fail(h, MMNB_ERR_CUDA, std::string("site gradients: ") + cudaGetErrorString(e));
+  // LJ tail: U_tail = cA totA + cB totB over the classes' (sigma, eps, count);
+  // d totA / d sig_i = 2 sum_b n_b dA_ab/dsig_a for site i in class a
+  if (h->cfg.include_lj_correction && (du_dsig || du_deps) && !h->cls_sig.empty()) {
+    const double cA = lj_tail_ab(h, 1, 0), cB = lj_tail_ab(h, 0, 1);
+    const size_t nc = h->cls_sig.size();
+    std::vector<double> ts(nc, 0.0), te(nc, 0.0);
+    for (size_t ca = 0; ca < nc; ca++)
+      for (size_t cb = 0; cb < nc; cb++) {
+        const double sa = h->cls_sig[ca], sb = h->cls_sig[cb], ea = h->cls_eps[ca], eb = h->cls_eps[cb];
+        const bool geo = h->cfg.geometric_combining_for_sigma != 0;
+        const double s6 = pow(geo ? sqrt(sa * sb) : 0.5 * (sa + sb), 6);
+        const double kap = geo ? 3 / sa : 6 / (sa + sb);
+        const double bb = 4 * sqrt(ea * eb) * s6, aa = bb * s6;
+        const double nb = (double) h->cls_n[cb];
+        ts[ca] += 2 * nb * (cA * 2 * kap * aa - cB * kap * bb);
+        if (ea > 0)
+          te[ca] += 2 * nb * (cA * aa - cB * bb) / (2 * ea);
+      }
+    for (size_t i = 0; i < n; i++) {
+      const int c = h->site_cls[i];
+      if (c < 0)
+        continue;
+      if (du_dsig)
+        du_dsig[i] += ts[c];
+      if (du_deps)
+        du_deps[i] += te[c];
+    }
   }
-  const bool tail = h->cfg.include_lj_correction != 0;
-  const double ta = tail ? lj_tail_ab(h, h->totA, 0) : 0, tb = tail ? lj_tail_ab(h, 0, h->totB) : 0;
-  grad_u[0] = 2 * en.elec;
-  grad_u[1] = 12 * (ea + ta) - 6 * eb + 6 * tb;
-  grad_u[2] = ea - eb + ta + tb;
-  if (grad_l) {
-    grad_l[0] = dl_df ? 2 * (gF - (ga - gb)) : 0;
-    grad_l[1] = dl_df ? 12 * ga - 6 * gb : 0;
-    grad_l[2] = dl_df ? ga - gb : 0;
+  return MMNB_OK;
+}
+
+extern "C" int mmnb_backward(mmnb_handle *h, const double *r, const double *dl_df, double *f, double *u,
+                             double grad_u[3], double grad_l[3])
+{
+  if (!h || !r || !grad_u)
+    return grad_fail(h, MMNB_ERR_ARG, "null handle, positions or gradient output");
+  int s = mmnb_forward(h, r, f, u, nullptr);
+  if (s)
+    return s;
+  const size_t n = h->nsite;
+  std::vector<double> g(6 * n, 0.0);
+  s = mmnb_site_gradients(h, dl_df, g.data(), g.data() + n, g.data() + 2 * n, g.data() + 3 * n, g.data() + 4 * n,
+                          g.data() + 5 * n);
+  if (s)
+    return s;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (size_t i = 0; i < n; i++) {
+    const double p[3] = {h->hq[i], h->hsig[i], h->heps[i]};
+    for (int k = 0; k < 6; k++)
+      acc[k] += p[k % 3] * g[k * n + i];
   }
-  if (f)
-    for (size_t k = 0; k < n3; k++)
-      f[k] += fw[k];
-  if (u)
-    *u += en.total;
+  for (int k = 0; k < 3; k++)
+    grad_u[k] = acc[k];
+  if (grad_l)
+    for (int k = 0; k < 3; k++)
+      grad_l[k] = dl_df ? acc[3 + k] : 0;
   return MMNB_OK;
 }

@@ -439,7 +439,7 @@ void free_all(mmnb_handle *h)
                   h->d_mesh, h->d_meshk, h->d_green, h->d_kvec, h->d_egrid, h->d_egridk, h->d_mesh32,
                   h->d_meshk32, h->d_green32, h->d_mesh_fx, h->d_kint, h->d_kvecs, h->d_ak, h->d_skc,
                   h->mx.site, h->mx.par, h->mx.anchor, h->mx.acc, h->mx.acck, h->d_wsum,
-                  h->d_bwd};
+                  h->d_bwd, h->d_gmesh, h->d_gmeshk};
   for (void *p : ptrs)
     if (p)
       cudaFree(p);
@@ -467,6 +467,10 @@ void free_all(mmnb_handle *h)
     cufftDestroy(h->plan_r2c32);
   if (h->plan_c2r32)
     cufftDestroy(h->plan_c2r32);
+  if (h->gplan_r2c)
+    cufftDestroy(h->gplan_r2c);
+  if (h->gplan_c2r)
+    cufftDestroy(h->gplan_c2r);
   for (auto e : h->timing.pool)
     cudaEventDestroy(e);
   if (h->graph_exec)
@@ -829,10 +833,16 @@ int mmnb_set_params(mmnb_handle *h, const int *site_mask, const double *q, const
   CK(cudaMemcpy(h->d_sig, sig, sizeof(double) * n, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(h->d_eps, eps, sizeof(double) * n, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(h->d_rscreen, rs.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+  h->grad_ready = false;
+  h->hq.assign(q, q + n);
+  h->hsig.assign(sig, sig + n);
+  h->heps.assign(eps, eps + n);
   // LJ tail totals over distinct (sigma, epsilon) printed as %12.6g
   // (src/eleclj.cpp:283-308)
-  struct T { double s, e; long n; };
-  std::vector<T> ty;
+  h->cls_sig.clear();
+  h->cls_eps.clear();
+  h->cls_n.clear();
+  h->site_cls.assign(n, -1);
   for (int i = 0; i < n; i++) {
     if (!(site_mask[i] & MMNB_SITE_HAS_LJ))
       continue;
@@ -841,18 +851,23 @@ int mmnb_set_params(mmnb_handle *h, const int *site_mask, const double *q, const
     snprintf(key, sizeof key, "%12.6g %12.6g", sig[i], eps[i]);
     sscanf(key, "%lf%lf", &sv, &ev);
     size_t a = 0;
-    for (; a < ty.size(); a++)
-      if (ty[a].s == sv && ty[a].e == ev)
+    for (; a < h->cls_sig.size(); a++)
+      if (h->cls_sig[a] == sv && h->cls_eps[a] == ev)
         break;
-    if (a == ty.size())
-      ty.push_back(T{sv, ev, 0});
-    ty[a].n++;
+    if (a == h->cls_sig.size()) {
+      h->cls_sig.push_back(sv);
+      h->cls_eps.push_back(ev);
+      h->cls_n.push_back(0);
+    }
+    h->cls_n[a]++;
+    h->site_cls[i] = (int) a;
   }
   h->totA = h->totB = 0;
-  for (auto &a : ty)
-    for (auto &b : ty) {
-      const double s6 = pow(h->cfg.geometric_combining_for_sigma ? sqrt(a.s * b.s) : 0.5 * (a.s + b.s), 6);
-      const double bb = 4 * sqrt(a.e * b.e) * a.n * b.n * s6;
+  for (size_t a = 0; a < h->cls_sig.size(); a++)
+    for (size_t b = 0; b < h->cls_sig.size(); b++) {
+      const double sa = h->cls_sig[a], sb = h->cls_sig[b];
+      const double s6 = pow(h->cfg.geometric_combining_for_sigma ? sqrt(sa * sb) : 0.5 * (sa + sb), 6);
+      const double bb = 4 * sqrt(h->cls_eps[a] * h->cls_eps[b]) * h->cls_n[a] * h->cls_n[b] * s6;
       h->totB -= bb;
       h->totA += bb * s6;
     }
@@ -872,6 +887,7 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
 {
   if (!h || !d_r)
     return fail(h, MMNB_ERR_ARG, "null handle or positions");
+  h->grad_ready = false;
   if (!h->params_set)
     return fail(h, MMNB_ERR_STATE, "mmnb_set_params has not been called");
   const bool mixed = h->cfg.precision == MMNB_MIXED;
@@ -1025,6 +1041,7 @@ int mmnb_graph_launch(mmnb_handle *h)
                 "device buffers were reallocated since the capture (rows regrown, mmnb_scale, mmnb_set_params): "
                 "capture again");
   CK(cudaGraphLaunch(h->graph_exec, h->stream));
+  h->grad_ready = false;
   h->evals++;
   h->launches += h->launch_per_eval;
   return MMNB_OK;
@@ -1042,10 +1059,14 @@ static void add_forces(double *f, const double *src, size_t b, size_t e)
     f[b + i] += src[b + i];
 }
 
-int mmnb_compute(mmnb_handle *h, const double *r, double *f, double *u, mmnb_energy *e, double *phi, double *evec)
+// keep: leave the site potentials and fields of this evaluation on the device
+// for mmnb_site_gradients (mmnb_forward)
+static int compute_host(mmnb_handle *h, const double *r, double *f, double *u, mmnb_energy *e, double *phi,
+                        double *evec, bool keep)
 {
   if (!h || !r)
     return fail(h, MMNB_ERR_ARG, "null handle or positions");
+  h->grad_ready = false;
   const size_t n3 = 3 * (size_t) h->nsite;
   if (!h->ev_flags) {
     CK(cudaEventCreateWithFlags(&h->ev_flags, cudaEventDisableTiming));
@@ -1056,7 +1077,8 @@ int mmnb_compute(mmnb_handle *h, const double *r, double *f, double *u, mmnb_ene
     CK(cudaMemcpyAsync(h->d_r, r, sizeof(double) * n3, cudaMemcpyHostToDevice, h->stream));
     // after the first call, a plain evaluation replays the handle's own graph
     // (zeroing, list check/rebuild, pair and mesh kernels, finalize)
-    const bool graph = !h->first && !(phi || evec) && !h->timing.on && !h->force_rebuild_next && !h->want_virial;
+    const bool graph =
+        !h->first && !(phi || evec || keep) && !h->timing.on && !h->force_rebuild_next && !h->want_virial;
     if (graph && !h->hgraph_exec) {
       CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
       h->capturing = true;
@@ -1088,7 +1110,7 @@ int mmnb_compute(mmnb_handle *h, const double *r, double *f, double *u, mmnb_ene
     } else {
       CK(cudaMemsetAsync(h->d_f, 0, sizeof(double) * n3, h->stream));
       CK(cudaMemsetAsync(h->d_flags + kFlagOverflow, 0, sizeof(int), h->stream));
-      h->want_fields = phi || evec;
+      h->want_fields = phi || evec || keep;
       const int s = mmnb_compute_device(h, h->d_r, h->d_f, h->d_energy);
       h->want_fields = false;
       if (s)
@@ -1151,9 +1173,20 @@ int mmnb_compute(mmnb_handle *h, const double *r, double *f, double *u, mmnb_ene
       e->lj_correction = h->h_out[2];
       e->total = h->h_out[3];
     }
+    h->grad_ready = keep;
     return MMNB_OK;
   }
   return fail(h, MMNB_ERR_OVERFLOW, "neighbour rows overflowed twice");
+}
+
+int mmnb_compute(mmnb_handle *h, const double *r, double *f, double *u, mmnb_energy *e, double *phi, double *evec)
+{
+  return compute_host(h, r, f, u, e, phi, evec, false);
+}
+
+int mmnb_forward(mmnb_handle *h, const double *r, double *f, double *u, mmnb_energy *e)
+{
+  return compute_host(h, r, f, u, e, nullptr, nullptr, true);
 }
 
 __global__ void k_scale_green(long nk, double s, double *green, double *kvec)
@@ -1184,6 +1217,7 @@ int mmnb_scale(mmnb_handle *h, double s)
                                           ", rspace_cutoff + neighbor_list_width would reach half the box");
   }
   drop_host_graph(h);
+  h->grad_ready = false;
   for (int d = 0; d < 3; d++) {
     h->box.L[d] *= s;
     h->box.invL[d] = 1 / h->box.L[d];

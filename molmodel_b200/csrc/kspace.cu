@@ -71,6 +71,75 @@ __global__ void k_kspace_field(int nsite, int nk, const double *__restrict__ r, 
   evec[3 * i + 2] += gz;
 }
 
+// Adjoint: sum_j q_j g_j . dE_j/dq_i for the reciprocal sum.  With
+// E_j = sum_k 2 a_k k (C sin k.r_j - S cos k.r_j) and C, S linear in the
+// charges, dE_j/dq_i = sum_k 2 a_k k sin(k.(r_j - r_i)), so the sum is
+// sum_k 2 a_k (Ds cos k.r_i - Dc sin k.r_i) with the dipole structure factor
+// Dc + i Ds = sum_j q_j (k . g_j) exp(i k.r_j).
+__global__ void k_kspace_dipole_structure(int nsite, int nk, const double *__restrict__ r,
+                                          const double *__restrict__ q, const double *__restrict__ g,
+                                          const double *__restrict__ kvec, double *__restrict__ skd)
+{
+  __shared__ double sc[kKThreads], ss[kKThreads];
+  const int k = blockIdx.x;
+  if (k >= nk)
+    return;
+  const double kx = kvec[3 * k], ky = kvec[3 * k + 1], kz = kvec[3 * k + 2];
+  double c = 0, s = 0;
+  for (int i = threadIdx.x; i < nsite; i += blockDim.x) {
+    double sn, cs;
+    sincos(kx * r[3 * i] + ky * r[3 * i + 1] + kz * r[3 * i + 2], &sn, &cs);
+    const double w = q[i] * (kx * g[3 * i] + ky * g[3 * i + 1] + kz * g[3 * i + 2]);
+    c += w * cs;
+    s += w * sn;
+  }
+  sc[threadIdx.x] = c;
+  ss[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      sc[threadIdx.x] += sc[threadIdx.x + w];
+      ss[threadIdx.x] += ss[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    skd[2 * k] = sc[0];
+    skd[2 * k + 1] = ss[0];
+  }
+}
+
+__global__ void k_kspace_dipole_potential(int nsite, int nk, const double *__restrict__ r,
+                                          const double *__restrict__ kvec, const double *__restrict__ ak,
+                                          const double *__restrict__ skd, double *__restrict__ psi)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nsite)
+    return;
+  const double x = r[3 * i], y = r[3 * i + 1], z = r[3 * i + 2];
+  double p = 0;
+  for (int k = 0; k < nk; k++) {
+    const double kx = __ldg(kvec + 3 * k), ky = __ldg(kvec + 3 * k + 1), kz = __ldg(kvec + 3 * k + 2);
+    double sn, cs;
+    sincos(kx * x + ky * y + kz * z, &sn, &cs);
+    p += 2 * __ldg(ak + k) * (__ldg(skd + 2 * k + 1) * cs - __ldg(skd + 2 * k) * sn);
+  }
+  psi[i] += p;
+}
+
+cudaError_t launch_kspace_dipole(mmnb_handle *h, const double *d_r, const double *d_g, double *d_skd,
+                                 double *d_psi)
+{
+  if (h->nk == 0)
+    return cudaSuccess;
+  k_kspace_dipole_structure<<<h->nk, kKThreads, 0, h->stream>>>(h->nsite, h->nk, d_r, h->d_q, d_g, h->d_kvecs,
+                                                                 d_skd);
+  k_kspace_dipole_potential<<<div_up(h->nsite, 128), 128, 0, h->stream>>>(h->nsite, h->nk, d_r, h->d_kvecs,
+                                                                          h->d_ak, d_skd, d_psi);
+  h->launches += 2;
+  return cudaGetLastError();
+}
+
 cudaError_t launch_kspace(mmnb_handle *h, const double *d_r)
 {
   if (h->nk == 0)

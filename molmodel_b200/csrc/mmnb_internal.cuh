@@ -195,8 +195,22 @@ struct mmnb_handle {
   // [3]: row counter of the FP64 water kernel; [4]: the mixed water kernel's
   // fixed-point virial term
   unsigned long long *d_wsum = nullptr;
-  double *d_bwd = nullptr;           // backward pass: row partials and dL/dF (allocated on first use)
+  // parameter gradients (allocated on first use): six per-site outputs, dL/dF,
+  // the dipole structure factor of the reciprocal sum
+  double *d_bwd = nullptr;
   size_t bwd_cap = 0;
+  bool grad_ready = false;           // the last evaluation was mmnb_forward's and nothing changed since
+  // FP64 dipole solve for a mixed-form handle, which has no FP64 meshes or plans
+  double *d_gmesh = nullptr;
+  cufftDoubleComplex *d_gmeshk = nullptr;
+  cufftHandle gplan_r2c = 0, gplan_c2r = 0;
+  // host copies of the site parameters, and the LJ classes of the tail:
+  // distinct (sigma, epsilon) as printed with %12.6g, their site counts, and
+  // each site's class (-1 without LJ)
+  std::vector<double> hq, hsig, heps;
+  std::vector<double> cls_sig, cls_eps;
+  std::vector<long> cls_n;
+  std::vector<int> site_cls;
   int lj_pair_blocks = 0, lj_excl_blocks = 0;
   double *d_elec_part = nullptr;     // per block
   int elec_blocks = 0;
@@ -273,6 +287,20 @@ cudaError_t launch_exclusions(mmnb_handle *h, const double *d_r);
 cudaError_t launch_p3m_green(mmnb_handle *h);
 // stage bit 1: spread + FFT round trip, bit 2: gather
 cudaError_t launch_p3m_fp64(mmnb_handle *h, const double *d_r, int stage);
+// FP64 meshes and plans of the adjoint's dipole solve: spread/spreadk hold one
+// mesh (three with ik differentiation); solvek/solve the summed ik spectrum
+// and its transform (ik only; otherwise the solve happens in place)
+struct P3mScratch {
+  double *spread = nullptr, *solve = nullptr;
+  cufftDoubleComplex *spreadk = nullptr, *solvek = nullptr;
+  cufftHandle r2c = 0, c2r = 0;
+};
+// d_psi += mesh potential of the dipoles q_j g_j (g: 3 per site), FP64
+cudaError_t launch_p3m_dipole_fp64(mmnb_handle *h, const double *d_r, const double *d_g, const P3mScratch &s,
+                                   double *d_psi);
+// d_psi += reciprocal-sum potential of the dipoles q_j g_j; d_skd: 2 per k
+cudaError_t launch_kspace_dipole(mmnb_handle *h, const double *d_r, const double *d_g, double *d_skd,
+                                 double *d_psi);
 cudaError_t launch_p3m_mixed(mmnb_handle *h, const double *d_r, int stage);
 cudaError_t launch_green32(mmnb_handle *h);
 cudaError_t launch_kspace(mmnb_handle *h, const double *d_r);
@@ -301,6 +329,42 @@ __device__ __forceinline__ bool csr_has(const int *ptr, const int *idx, int row,
       return true;
   }
   return false;
+}
+
+// b0 = erfc(eta r)/r, b1 = (b0 + 2 eta/sqrt(pi) exp(-eta^2 r^2)) / r^2 from the
+// reference's 512-segment Chebyshev table (8 doubles per segment) inside
+// (cmin, cmax), from erfc/exp outside it; seg and f: the table segment and the
+// position in it (seg = -1 outside the table)
+__device__ __forceinline__ void ewald_table_b(const double *cheb, double cmin, double cmax, double inv_dx,
+                                              double eta, double r2, double &b0, double &b1, int &seg, double &f)
+{
+  if (cmin < r2 && r2 < cmax) {
+    double x = (r2 - cmin) * inv_dx;
+    const unsigned i = (unsigned) x;
+    const double2 *c = reinterpret_cast<const double2 *>(cheb + 8 * (size_t) i);
+    const double2 c01 = __ldg(c), c23 = __ldg(c + 1), c45 = __ldg(c + 2), c67 = __ldg(c + 3);
+    x -= i;
+    b0 = ((c23.y * x + c23.x) * x + c01.y) * x + c01.x;
+    b1 = (c67.x * x + c45.y) * x + c45.x;
+    seg = (int) i;
+    f = x;
+  } else {
+    const double r = sqrt(r2);
+    const double er = eta * r;
+    const double e = exp(-(er * er));
+    b0 = erfc(er) / r;
+    b1 = (b0 + eta * M_2_SQRTPI * e) / r2;
+    seg = -1;
+    f = 0;
+  }
+}
+
+// minimum image of one site displacement, rounded as the reference rounds it
+__device__ __forceinline__ void min_image_ref(const Box &b, double &x, double &y, double &z)
+{
+  x = __dadd_rn(x, __dmul_rn(-b.L[0], floor(__dadd_rn(__dmul_rn(x, b.invL[0]), 0.5))));
+  y = __dadd_rn(y, __dmul_rn(-b.L[1], floor(__dadd_rn(__dmul_rn(y, b.invL[1]), 0.5))));
+  z = __dadd_rn(z, __dmul_rn(-b.L[2], floor(__dadd_rn(__dmul_rn(z, b.invL[2]), 0.5))));
 }
 
 // anchor displacement with the reference's minimum-image rounding

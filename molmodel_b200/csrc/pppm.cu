@@ -385,6 +385,173 @@ cudaError_t launch_p3m_fp64(mmnb_handle *h, const double *d_r, int stage)
   }
 }
 
+// ---- adjoint: the mesh potential of a dipole density ------------------------
+//
+// For a loss L of the forces, dL/dq_i holds, besides g_i . E_i (g = dL/dF),
+// sum_j q_j g_j . dE_j/dq_i: the potential at r_i of point dipoles
+// p_j = q_j g_j, as the mesh sees them.  The map "charges -> mesh field at the
+// sites" is spread, solve, gather; its transpose runs the three steps
+// backwards with each one transposed:
+//   * real-space differentiation: E_j gathers the mesh potential with the
+//     vector weights A^T (-grad_s W)(r_j), and the solve (real, even influence
+//     function) is symmetric, so the dipoles are spread with those vector
+//     weights, solved with the same influence function and gathered with the
+//     plain weights W;
+//   * ik differentiation: E_j,d gathers C2R(-i k_d G rho^) with W; that
+//     operator is real and odd, its transpose C2R(+i k_d G .), so the three
+//     dipole components are spread with W and the solve sums
+//     i k_d G D^_d over d into one mesh.
+
+template <int P>
+__global__ void k_spread_dipole_fp64(MeshArgs m, const double *__restrict__ r, const double *__restrict__ q,
+                                     const int *__restrict__ mask, const double *__restrict__ g, int ik, size_t nr,
+                                     double *__restrict__ mesh)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nsite)
+    return;
+  const double qi = q[i];
+  if (!(mask[i] & MMNB_SITE_HAS_Q) || qi == 0)
+    return;
+  const double px = qi * g[3 * i], py = qi * g[3 * i + 1], pz = qi * g[3 * i + 2];
+  const double x = r[3 * i], y = r[3 * i + 1], z = r[3 * i + 2];
+  double W[3][P], ND[3][P];
+  int base[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const double s = m.A[d] * x + m.A[3 + d] * y + m.A[6 + d] * z;
+    base[d] = bspline_weights<P>(s, W[d], ND[d]);
+  }
+  int iy_[P], iz_[P];
+#pragma unroll
+  for (int p = 0; p < P; p++) {
+    iy_[p] = wrap_idx(base[1] + p, m.n[1]);
+    iz_[p] = wrap_idx(base[2] + p, m.n[2]);
+  }
+  // p . A^T v = (A p) . v for the vector weight v of the gather
+  const double c0 = m.A[0] * px + m.A[3] * py + m.A[6] * pz;
+  const double c1 = m.A[1] * px + m.A[4] * py + m.A[7] * pz;
+  const double c2 = m.A[2] * px + m.A[5] * py + m.A[8] * pz;
+  for (int a = 0; a < P; a++) {
+    const int ix = wrap_idx(base[0] + a, m.n[0]);
+#pragma unroll
+    for (int b = 0; b < P; b++) {
+      const size_t rowoff = ((size_t) ix * m.n[1] + iy_[b]) * m.n[2];
+#pragma unroll
+      for (int c = 0; c < P; c++) {
+        const size_t k = rowoff + iz_[c];
+        if (ik) {
+          const double w = W[0][a] * W[1][b] * W[2][c];
+          atomicAdd(mesh + k, px * w);
+          atomicAdd(mesh + nr + k, py * w);
+          atomicAdd(mesh + 2 * nr + k, pz * w);
+        } else {
+          atomicAdd(mesh + k, c0 * ND[0][a] * W[1][b] * W[2][c] + c1 * W[0][a] * ND[1][b] * W[2][c] +
+                                  c2 * W[0][a] * W[1][b] * ND[2][c]);
+        }
+      }
+    }
+  }
+}
+
+// ik: out = G sum_d i k_d D^_d
+__global__ void k_dipole_green_ik(long nk, const double *__restrict__ green, const double *__restrict__ kvec,
+                                  const cufftDoubleComplex *__restrict__ dk, cufftDoubleComplex *__restrict__ out)
+{
+  const long g = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nk)
+    return;
+  double re = 0, im = 0;
+  for (int d = 0; d < 3; d++) {
+    const double k = kvec[3 * g + d];
+    const cufftDoubleComplex v = dk[d * nk + g];
+    re -= k * v.y;
+    im += k * v.x;
+  }
+  const double a = green[g];
+  out[g] = make_cuDoubleComplex(a * re, a * im);
+}
+
+template <int P>
+__global__ void k_gather_potential_fp64(MeshArgs m, const double *__restrict__ r, const double *__restrict__ mesh,
+                                        double *__restrict__ out)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nsite)
+    return;
+  const double x = r[3 * i], y = r[3 * i + 1], z = r[3 * i + 2];
+  double W[3][P], ND[3][P];
+  int base[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const double s = m.A[d] * x + m.A[3 + d] * y + m.A[6 + d] * z;
+    base[d] = bspline_weights<P>(s, W[d], ND[d]);
+  }
+  int iy_[P], iz_[P];
+#pragma unroll
+  for (int p = 0; p < P; p++) {
+    iy_[p] = wrap_idx(base[1] + p, m.n[1]);
+    iz_[p] = wrap_idx(base[2] + p, m.n[2]);
+  }
+  double ph = 0;
+  for (int a = 0; a < P; a++) {
+    const int ix = wrap_idx(base[0] + a, m.n[0]);
+#pragma unroll
+    for (int b = 0; b < P; b++) {
+      const size_t rowoff = ((size_t) ix * m.n[1] + iy_[b]) * m.n[2];
+      const double wxy = W[0][a] * W[1][b];
+#pragma unroll
+      for (int c = 0; c < P; c++)
+        ph += wxy * W[2][c] * __ldg(mesh + rowoff + iz_[c]);
+    }
+  }
+  out[i] += ph;
+}
+
+template <int P>
+static cudaError_t p3m_dipole_p(mmnb_handle *h, const double *d_r, const double *d_g, const P3mScratch &s,
+                                double *d_psi)
+{
+  const MeshArgs m = mesh_args(h);
+  const size_t nr = (size_t) h->mesh[0] * h->mesh[1] * h->mesh[2];
+  const long nk = (long) h->mesh[0] * h->mesh[1] * (h->mesh[2] / 2 + 1);
+  const int ik = h->cfg.p3m_ik_differentiate ? 1 : 0;
+  const int nmesh = ik ? 3 : 1;
+  cudaError_t e = cudaMemsetAsync(s.spread, 0, sizeof(double) * nr * nmesh, h->stream);
+  if (e != cudaSuccess)
+    return e;
+  k_spread_dipole_fp64<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->d_q, h->d_mask, d_g, ik, nr,
+                                                                         s.spread);
+  if (cufftSetStream(s.r2c, h->stream) != CUFFT_SUCCESS || cufftSetStream(s.c2r, h->stream) != CUFFT_SUCCESS)
+    return cudaErrorUnknown;
+  for (int d = 0; d < nmesh; d++)
+    if (cufftExecD2Z(s.r2c, s.spread + d * nr, s.spreadk + d * nk) != CUFFT_SUCCESS)
+      return cudaErrorUnknown;
+  if (ik)
+    k_dipole_green_ik<<<div_up(nk, 256), 256, 0, h->stream>>>(nk, h->d_green, h->d_kvec, s.spreadk, s.solvek);
+  else
+    k_green_mul<<<div_up(nk, 256), 256, 0, h->stream>>>(nk, h->d_green, s.spreadk, h->d_kvec, nullptr);
+  if (cufftExecZ2D(s.c2r, ik ? s.solvek : s.spreadk, s.solve) != CUFFT_SUCCESS)
+    return cudaErrorUnknown;
+  k_gather_potential_fp64<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, s.solve, d_psi);
+  h->launches += 3;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_p3m_dipole_fp64(mmnb_handle *h, const double *d_r, const double *d_g, const P3mScratch &s,
+                                   double *d_psi)
+{
+  switch (h->cfg.p3m_assignment_order) {
+  case 2: return p3m_dipole_p<2>(h, d_r, d_g, s, d_psi);
+  case 3: return p3m_dipole_p<3>(h, d_r, d_g, s, d_psi);
+  case 4: return p3m_dipole_p<4>(h, d_r, d_g, s, d_psi);
+  case 5: return p3m_dipole_p<5>(h, d_r, d_g, s, d_psi);
+  case 6: return p3m_dipole_p<6>(h, d_r, d_g, s, d_psi);
+  case 7: return p3m_dipole_p<7>(h, d_r, d_g, s, d_psi);
+  default: return cudaErrorInvalidValue;
+  }
+}
+
 // ---- mixed form: FP32 weights, 64-bit fixed-point mesh, FP32 FFT -------------
 //
 // Charge assignment accumulates q w_x w_y w_z in 64-bit fixed point

@@ -51,25 +51,7 @@ struct PairArgs {
 // f: the table segment and the position in it (seg = -1 outside the table)
 __device__ __forceinline__ void ewald_b(const PairArgs &a, double r2, double &b0, double &b1, int &seg, double &f)
 {
-  if (a.cheb_min < r2 && r2 < a.cheb_max) {
-    double x = (r2 - a.cheb_min) * a.cheb_inv_dx;
-    const unsigned i = (unsigned) x;
-    const double2 *c = reinterpret_cast<const double2 *>(a.cheb + 8 * (size_t) i);
-    const double2 c01 = __ldg(c), c23 = __ldg(c + 1), c45 = __ldg(c + 2), c67 = __ldg(c + 3);
-    x -= i;
-    b0 = ((c23.y * x + c23.x) * x + c01.y) * x + c01.x;
-    b1 = (c67.x * x + c45.y) * x + c45.x;
-    seg = (int) i;
-    f = x;
-  } else {
-    const double r = sqrt(r2);
-    const double er = a.eta * r;
-    const double e = exp(-(er * er));
-    b0 = erfc(er) / r;
-    b1 = (b0 + a.eta * M_2_SQRTPI * e) / r2;
-    seg = -1;
-    f = 0;
-  }
+  ewald_table_b(a.cheb, a.cheb_min, a.cheb_max, a.cheb_inv_dx, a.eta, r2, b0, b1, seg, f);
 }
 
 // The table is refitted for each eta, so along the volume-move path its eta
@@ -354,13 +336,6 @@ struct ExclArgs {
   double *lj14_part;
   double *vir14_part;  // per block: the 1-4 LJ force scalars times r^2 / 2 (mmnb_virial), or null
 };
-
-__device__ __forceinline__ void min_image_ref(const Box &b, double &x, double &y, double &z)
-{
-  x = __dadd_rn(x, __dmul_rn(-b.L[0], floor(__dadd_rn(__dmul_rn(x, b.invL[0]), 0.5))));
-  y = __dadd_rn(y, __dmul_rn(-b.L[1], floor(__dadd_rn(__dmul_rn(y, b.invL[1]), 0.5))));
-  z = __dadd_rn(z, __dmul_rn(-b.L[2], floor(__dadd_rn(__dmul_rn(z, b.invL[2]), 0.5))));
-}
 
 __global__ void __launch_bounds__(kExclThreads) k_exclusions_fp64(ExclArgs a)
 {

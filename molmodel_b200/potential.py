@@ -132,6 +132,33 @@ class ElecLJ:
             out.update(phi=phi, evec=evec)
         return out
 
+    # ---- adjoint --------------------------------------------------------------
+    def forward(self, r):
+        """mmnb_forward: compute() that keeps on the device what
+        site_gradients() needs.  Returns compute()'s dict."""
+        lib = load()
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        f = np.zeros((self.nsite, 3))
+        e = MmnbEnergy()
+        check(lib.mmnb_forward(self._h, _d(r), _d(f), None, ctypes.byref(e)), self._h)
+        self.energy = dict(elec=e.elec, lj=e.lj, lj_correction=e.lj_correction, total=e.total)
+        return dict(f=f, **self.energy)
+
+    def site_gradients(self, dl_df=None):
+        """mmnb_site_gradients for the last forward(): per-site arrays du_dq,
+        du_dsig, du_deps (dU/dq_i, dU/dsigma_i, dU/depsilon_i) and, given
+        dl_df = dL/dF (nsite x 3), dl_dq, dl_dsig, dl_deps for that loss."""
+        n = self.nsite
+        out = {k: np.zeros(n) for k in ("du_dq", "du_dsig", "du_deps")}
+        g = None
+        if dl_df is not None:
+            g = np.ascontiguousarray(dl_df, dtype=np.float64).reshape(n, 3)
+            out.update({k: np.zeros(n) for k in ("dl_dq", "dl_dsig", "dl_deps")})
+        check(load().mmnb_site_gradients(self._h, _d(g), _d(out["du_dq"]), _d(out["du_dsig"]),
+                                         _d(out["du_deps"]), _d(out.get("dl_dq")), _d(out.get("dl_dsig")),
+                                         _d(out.get("dl_deps"))), self._h)
+        return out
+
     def electrostatic_potential_at_gridpoints(self, r, points):
         """ElecLJ::electrostatic_potential_at_gridpoints (src/eleclj.cpp:1302-1340):
         potential of the sites at r (nsite x 3) at each point (npoint x 3), in

@@ -1,71 +1,259 @@
-"""Adjoint (mmnb_backward) for the water parameters (q_O, sigma_O, epsilon_O):
-gradients of the total energy and of a force-matching loss against central
-finite differences of the FP64 oracle (relative step 1e-4), for the FP64 and
-the mixed forward."""
+"""Adjoint (mmnb_forward, then mmnb_site_gradients): per-site gradients of the
+energy U and of a force-matching loss L = sum_i |F_i - F_i^target|^2 with
+respect to site charges, sigmas and epsilons, against central differences of
+the oracle's energy and forces.
+
+Directional checks: for a seeded direction v over the sites, sum_i v_i dX/dp_i
+against (X(p + h v) - X(p - h v)) / 2h, Richardson-extrapolated over h and 2h,
+with X = U or L and p = q, sigma or epsilon.  The charge directions are
+non-uniform (random per site, or on one site type only), which a gradient with
+respect to a uniform charge scale could not answer.  Positions do not move, so
+no table segment join is crossed.  The sigma and epsilon steps are multiples of
+1e-4 and 1e-5, exact in the six significant digits the reference's LJ tail
+keys on (src/eleclj.cpp:283-308).
+
+Systems: rigid water with the Ewald k-sum, P3M with real-space and with ik
+differentiation, and a water box with cross-group exclusions, screening
+radii, 1-4 pairs (O-O and O-H, scaled) and LJ on the H sites, so that every
+term of the backward pass runs.  The C5 case (512 waters, 64 frames 1 ps apart
+from FP64 dynamics at 300 K) checks the water-parameter gradients
+d/d(q_O, sigma_O, epsilon_O) and a force-matching fit driven by them.
+"""
 import numpy as np
 import pytest
 
 from molmodel_b200 import ElecLJ, maxwell_boltzmann, water_box
-from molmodel_b200.adjoint import water_fit_gradients
+from molmodel_b200._lib import MmnbError
+from molmodel_b200.adjoint import (backward, fit_water, type_gradients, water_fit_gradients, water_site_params,
+                                   water_site_types)
 from molmodel_b200.md import MDyn
-from molmodel_b200.units import e_to_charge_unit
-from molmodel_b200.water import EPSILON_O, Q_O_E, SIGMA_O
+from molmodel_b200.water import EPSILON_O, Q_O_E, SIGMA_O, SITE_HAS_LJ, SITE_HAS_Q
 from oracle.oracle import make_config, port
 
 pytestmark = pytest.mark.gpu
 
-
-def _params(wb, theta):
-    q_o, s_o, e_o = theta
-    q = np.tile([q_o, -q_o / 2, -q_o / 2], wb.nwater)
-    sig = np.zeros(wb.nsite)
-    eps = np.zeros(wb.nsite)
-    sig[0::3] = s_o
-    eps[0::3] = e_o
-    return e_to_charge_unit(q), sig, eps
+MMNB_ERR_STATE = 6
 
 
-def _oracle(wb, cfg, theta):
-    q, sig, eps = _params(wb, theta)
-    return port().eleclj(make_config(wb.box, **cfg), wb.nsite, wb.groups, wb.exclusions, wb.site_mask, q, sig, eps,
-                         wb.rscreen)
+class System:
+    """Site arrays of a water box, optionally with the extra terms."""
+
+    def __init__(self, wb, extra=False, seed=3):
+        self.nsite, self.box, self.positions = wb.nsite, wb.box, wb.positions
+        self.groups, self.exclusions = wb.groups, wb.exclusions
+        self.site_mask = wb.site_mask.copy()
+        self.q, self.sigma, self.epsilon = wb.q.copy(), wb.sigma.copy(), wb.epsilon.copy()
+        self.rscreen = np.zeros(wb.nsite)
+        self.pairs14 = None
+        if extra:
+            rng = np.random.default_rng(seed)
+            n = wb.nwater
+            k = rng.choice(n - 1, size=n // 4, replace=False)
+            more = np.concatenate([np.stack([3 * k, 3 * (k + 1)], 1), np.stack([3 * k + 1, 3 * (k + 1) + 2], 1)])
+            self.exclusions = np.concatenate([wb.exclusions, more]).astype(np.int32)
+            self.rscreen = np.where(np.arange(wb.nsite) % 3 == 0, 1.6, 0.0)
+            j = rng.choice(n - 3, size=n // 5, replace=False)
+            self.pairs14 = np.concatenate([np.stack([3 * j, 3 * (j + 2)], 1),
+                                           np.stack([3 * j, 3 * (j + 3) + 1], 1)]).astype(np.int32)
+            h = np.arange(wb.nsite) % 3 != 0
+            self.site_mask = np.full(wb.nsite, SITE_HAS_Q | SITE_HAS_LJ, dtype=np.int32)
+            self.sigma = np.where(h, 1.0, self.sigma)
+            self.epsilon = np.where(h, 0.01, self.epsilon)
+
+
+def oracle_eval(s, cfg, q=None, sig=None, eps=None):
+    o = port().eleclj(make_config(s.box, **cfg), s.nsite, s.groups, s.exclusions, s.site_mask,
+                      s.q if q is None else q, s.sigma if sig is None else sig, s.epsilon if eps is None else eps,
+                      s.rscreen, pairs14=s.pairs14)
+    return o.eval(s.positions)
+
+
+def directional_fd(s, cfg, which, v, h, targets):
+    """Richardson-extrapolated central differences of U and L along v."""
+    base = dict(q=s.q, sig=s.sigma, eps=s.epsilon)
+
+    def at(t):
+        p = dict(base)
+        p[which] = base[which] + t * v
+        out = oracle_eval(s, cfg, **p)
+        return out["total"], float(((out["f"] - targets) ** 2).sum())
+
+    d = []
+    for hh in (h, 2 * h):
+        (up, lp), (um, lm) = at(hh), at(-hh)
+        d.append(((up - um) / (2 * hh), (lp - lm) / (2 * hh)))
+    return tuple((4 * d[0][k] - d[1][k]) / 3 for k in range(2))
+
+
+def directions(s, rng):
+    """(name, parameter, direction, step) for the checks."""
+    qm = (s.site_mask & SITE_HAS_Q) != 0
+    lm = (s.site_mask & SITE_HAS_LJ) != 0
+    hsite = np.arange(s.nsite) % 3 != 0
+    out = [
+        ("q-random", "q", np.where(qm, rng.normal(size=s.nsite), 0.0), 1e-3),
+        ("q-H-only", "q", np.where(qm & hsite, rng.normal(size=s.nsite), 0.0), 1e-3),
+        ("q-one-site", "q", np.eye(s.nsite)[4], 1e-3),
+        ("sigma", "sig", np.where(lm, rng.integers(-2, 3, size=s.nsite), 0).astype(float), 1e-4),
+        ("epsilon", "eps", np.where(lm, rng.integers(-2, 3, size=s.nsite), 0).astype(float), 1e-5),
+    ]
+    return out
+
+
+CFG = dict(rspace_cutoff=9.0, smoothing_width=1.0, ewald_screening=0.35)
+CASES = [
+    ("ksum", False, dict(CFG, kspace_cutoff=7.0)),
+    ("p3m", False, dict(CFG, use_p3m=True, p3m_grid_spacing=18.63 / 20, p3m_assignment_order=5)),
+    ("p3m-ik", False, dict(CFG, use_p3m=True, p3m_grid_spacing=18.63 / 20, p3m_assignment_order=4,
+                           p3m_ik_differentiate=True)),
+    ("general", True, dict(CFG, kspace_cutoff=7.0, elec_1_4_scale_factor=0.5, lj_1_4_scale_factor=0.7)),
+    ("general-p3m", True, dict(CFG, use_p3m=True, p3m_grid_spacing=18.63 / 20, p3m_assignment_order=5,
+                               elec_1_4_scale_factor=0.5, lj_1_4_scale_factor=0.7)),
+]
+
+
+def grad_key(which):
+    return {"q": "dq", "sig": "dsig", "eps": "deps"}[which]
+
+
+@pytest.fixture(scope="module", params=CASES, ids=[c[0] for c in CASES])
+def case(request):
+    name, extra, cfg = request.param
+    wb = water_box(6, seed=11)
+    s = System(wb, extra)
+    # targets: the forces with every charge x 1.04 and the O sigmas + 0.03
+    tq = s.q * 1.04
+    tsig = np.where(np.arange(s.nsite) % 3 == 0, s.sigma + 0.03, s.sigma)
+    targets = oracle_eval(s, cfg, q=tq, sig=tsig)["f"]
+    rng = np.random.default_rng(5)
+    checks = []
+    for label, which, v, h in directions(s, rng):
+        fd_u, fd_l = directional_fd(s, cfg, which, v, h, targets)
+        checks.append((label, which, v, fd_u, fd_l))
+    return name, s, cfg, targets, checks
+
+
+def site_grads(s, cfg, precision, targets, dl_df=None):
+    p = ElecLJ(precision=precision, **cfg).init(s, pairs14=s.pairs14)
+    out = p.forward(s.positions)
+    g = p.site_gradients(2 * (out["f"] - targets) if dl_df is None else dl_df)
+    p.close()
+    return out, g
+
+
+def test_fp64_site_gradients_match_finite_differences(case):
+    name, s, cfg, targets, checks = case
+    out, g = site_grads(s, cfg, "fp64", targets)
+    for label, which, v, fd_u, fd_l in checks:
+        k = grad_key(which)
+        pu = float(v @ g["du_" + k])
+        pl = float(v @ g["dl_" + k])
+        assert abs(pu - fd_u) <= 3e-8 * abs(fd_u) + 1e-9, (name, label, pu, fd_u)
+        assert abs(pl - fd_l) <= 3e-8 * abs(fd_l) + 1e-9, (name, label, pl, fd_l)
+
+
+def test_mixed_site_gradients_match_fp64_for_the_same_loss_gradient(case):
+    """The mixed form's backward, given the same dL/dF, differs from the FP64
+    one only through the forward's site potentials and fields (FP32 pair
+    arithmetic): 2e-5 of the largest term."""
+    name, s, cfg, targets, checks = case
+    if cfg.get("p3m_ik_differentiate"):
+        pytest.skip("ik differentiation is FP64 only")
+    out64, g64 = site_grads(s, cfg, "fp64", targets)
+    dl_df = 2 * (out64["f"] - targets)
+    _, gm = site_grads(s, cfg, "mixed", targets, dl_df=dl_df)
+    for key in ("du_dq", "du_dsig", "du_deps", "dl_dq", "dl_dsig", "dl_deps"):
+        scale = np.abs(g64[key]).max()
+        assert np.abs(gm[key] - g64[key]).max() <= 2e-5 * scale, (name, key)
+
+
+def test_uniform_scale_backward_is_the_contracted_site_gradients():
+    wb = water_box(6, seed=12)
+    s = System(wb)
+    cfg = CASES[1][2]
+    targets = oracle_eval(s, cfg, q=s.q * 1.02)["f"]
+    p = ElecLJ(precision="fp64", **cfg).init(s)
+    out = p.forward(s.positions)
+    dl_df = 2 * (out["f"] - targets)
+    g = p.site_gradients(dl_df)
+    f, u, gu, gl = backward(p, s.positions, dl_df)
+    p.close()
+    assert abs(gu[0] - 2 * out["elec"]) <= 1e-10 * abs(out["elec"])
+    for k, (par, key) in enumerate(((s.q, "dq"), (s.sigma, "dsig"), (s.epsilon, "deps"))):
+        # bounded by the sum of the terms' sizes (the targets move only the
+        # charges, so the loss's sigma sum nearly cancels)
+        assert abs(gu[k] - par @ g["du_" + key]) <= 1e-12 * (np.abs(par * g["du_" + key]).sum())
+        assert abs(gl[k] - par @ g["dl_" + key]) <= 1e-12 * (np.abs(par * g["dl_" + key]).sum())
+    # the same forward again (the FP64 mesh is summed with atomic adds, so to rounding)
+    assert np.abs(f - out["f"]).max() <= 1e-12 * np.abs(out["f"]).max()
+    assert abs(u - out["total"]) <= 1e-12 * abs(out["total"])
+
+
+def test_site_gradients_need_the_forward_of_the_same_state():
+    wb = water_box(6, seed=13)
+    p = ElecLJ(precision="fp64", **CASES[1][2]).init(wb)
+    with pytest.raises(MmnbError) as ex:
+        p.site_gradients()
+    assert ex.value.status == MMNB_ERR_STATE
+    p.forward(wb.positions)
+    p.site_gradients()
+    p.compute(wb.positions)  # another evaluation discards the forward's state
+    with pytest.raises(MmnbError) as ex:
+        p.site_gradients()
+    assert ex.value.status == MMNB_ERR_STATE
+    p.forward(wb.positions)
+    p.set_params(wb.site_mask, wb.q, wb.sigma, wb.epsilon)
+    with pytest.raises(MmnbError) as ex:
+        p.site_gradients()
+    assert ex.value.status == MMNB_ERR_STATE
+    p.close()
+
+
+# ---- C5: the water parameters over 64 frames ---------------------------------
+
+C5_CFG = dict(rspace_cutoff=9.0, ewald_screening=0.35, use_p3m=True, p3m_assignment_order=5,
+              neighbor_list_width=1.0)
+
+
+def _water_oracle(wb, cfg, theta):
+    q, sig, eps = water_site_params(theta, wb.nwater)
+    return port().eleclj(make_config(wb.box, **cfg), wb.nsite, wb.groups, wb.exclusions, wb.site_mask, q, sig,
+                         eps, wb.rscreen)
 
 
 @pytest.fixture(scope="module")
-def case():
-    """512 waters (L 24.86 A), P3M 24^3; three frames 40 fs apart from FP64
-    dynamics at 300 K; targets from the perturbed parameters (q_O x 1.05,
-    sigma_O + 0.02 A, epsilon_O x 0.95)."""
+def c5():
+    """512 waters (L 24.86 A), P3M 24^3; 64 frames 1 ps apart from FP64
+    dynamics at 300 K (1 fs steps); targets from the perturbed parameters
+    (q_O x 1.05, sigma_O + 0.02 A, epsilon_O x 0.95)."""
     wb = water_box(8, seed=3)
-    cfg = dict(rspace_cutoff=9.0, ewald_screening=0.35, use_p3m=True, p3m_grid_spacing=wb.box / 24,
-               p3m_assignment_order=5, neighbor_list_width=1.0)
+    cfg = dict(C5_CFG, p3m_grid_spacing=wb.box / 24)
     pot = ElecLJ(precision="fp64", **cfg).init(wb)
     md = MDyn(pot, wb.masses, timestep=0.001)
     md.set_state(wb.positions, maxwell_boltzmann(wb, 300.0, seed=5))
     frames = []
-    for _ in range(3):
-        md.run(40)
+    for _ in range(64):
+        md.run(1000)
         frames.append(md.state()[0])
     md.close()
     pot.close()
     theta0 = np.array([Q_O_E, SIGMA_O, EPSILON_O])
     target_theta = np.array([Q_O_E * 1.05, SIGMA_O + 0.02, EPSILON_O * 0.95])
-    ot = _oracle(wb, cfg, target_theta)
+    ot = _water_oracle(wb, cfg, target_theta)
     targets = [ot.eval(r)["f"] for r in frames]
-    # central differences of L and U on the oracle
+
     def lu(theta):
-        o = _oracle(wb, cfg, theta)
+        o = _water_oracle(wb, cfg, theta)
         L = U = 0.0
         for r, ft in zip(frames, targets):
             out = o.eval(r)
             L += float(((out["f"] - ft) ** 2).sum())
             U += out["total"]
         return L, U
-    # central differences with relative steps of about 1e-4 (and twice that,
-    # combined by Richardson extrapolation so the O(h^2) truncation error of
-    # the quadratic loss drops out), rounded to one significant digit: the
-    # reference keys the LJ tail on sigma and epsilon printed with %12.6g
-    # (src/eleclj.cpp:283-308), so theta +- h must stay exact in six digits
+
+    # relative steps of about 1e-4 (and twice that, Richardson-extrapolated),
+    # rounded to one significant digit so theta +- h stays exact in the six
+    # digits the LJ tail keys on
     steps = [float(f"{1e-4 * abs(t):.0e}") for t in theta0]
     fd_l, fd_u = np.zeros(3), np.zeros(3)
     for k in range(3):
@@ -79,17 +267,55 @@ def case():
         fd_l[k] = (4 * d[0][0] - d[1][0]) / 3
         fd_u[k] = (4 * d[0][1] - d[1][1]) / 3
     L0, U0 = lu(theta0)
-    return wb, cfg, frames, targets, theta0, fd_l, fd_u, L0, U0
+    return wb, cfg, frames, targets, theta0, target_theta, fd_l, fd_u, L0, U0
 
 
-@pytest.mark.parametrize("precision,tol", [("fp64", 1e-6), ("mixed", 2e-3)])
-def test_gradients_match_finite_differences(case, precision, tol):
-    wb, cfg, frames, targets, theta0, fd_l, fd_u, L0, U0 = case
+# the mixed forward's forces carry ~4e-6 relative error, and the loss
+# gradient inherits it through dL/dF = 2 (F - F^target), where F - F^target
+# is ~5% of F: ~1e-4 relative
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-7), ("mixed", 3e-4)])
+def test_c5_water_parameter_gradients(c5, precision, tol):
+    wb, cfg, frames, targets, theta0, _, fd_l, fd_u, L0, U0 = c5
     pot = ElecLJ(precision=precision, **cfg).init(wb)
-    L, dl, U, du = water_fit_gradients(pot, frames, targets, theta0)
+    L, dl, U, du = water_fit_gradients(pot, frames, targets)
     pot.close()
-    assert abs(L - L0) < 1e-6 * L0 if precision == "fp64" else abs(L - L0) < 1e-3 * L0
-    assert abs(U - U0) < 1e-9 * abs(U0) if precision == "fp64" else abs(U - U0) < 1e-4 * abs(U0)
+    assert abs(L - L0) < (1e-8 if precision == "fp64" else 1e-3) * L0
+    assert abs(U - U0) < (1e-10 if precision == "fp64" else 5e-5) * abs(U0)
     for k in range(3):
-        assert abs(du[k] - fd_u[k]) <= tol * abs(fd_u[k]) + 1e-9 * abs(U0), (k, du, fd_u)
+        assert abs(du[k] - fd_u[k]) <= tol * abs(fd_u[k]), (k, du, fd_u)
         assert abs(dl[k] - fd_l[k]) <= tol * abs(fd_l[k]), (k, dl, fd_l)
+
+
+def test_c5_one_evaluation_per_frame(c5):
+    wb, cfg, frames, targets = c5[:4]
+    pot = ElecLJ(precision="fp64", **cfg).init(wb)
+    pot.compute(frames[0])
+    before = pot.counters()
+    water_fit_gradients(pot, frames[:8], targets[:8])
+    after = pot.counters()
+    pot.close()
+    assert after[1] - before[1] == 8  # evaluations counted by the device
+
+
+def test_c5_type_gradients_sum_the_sites(c5):
+    wb, cfg, frames, targets = c5[:4]
+    pot = ElecLJ(precision="fp64", **cfg).init(wb)
+    out = pot.forward(frames[0])
+    g = pot.site_gradients(2 * (out["f"] - targets[0]))
+    pot.close()
+    t = type_gradients(g, water_site_types(wb.nwater), "du")
+    assert set(t) == {"O", "H"}
+    assert t["H"][1] == 0 and t["H"][2] == 0  # no LJ on H
+    # dU/dq_type . q_type over the types = 2 U_elec (charges in e)
+    q_o, q_h = Q_O_E, -Q_O_E / 2
+    assert abs(t["O"][0] * q_o + t["H"][0] * q_h - 2 * out["elec"]) <= 1e-10 * abs(out["elec"])
+
+
+def test_c5_force_matching_fit_recovers_the_target_parameters(c5):
+    """L-BFGS on the adjoint gradients from theta0 to the parameters the
+    targets were made with (8 of the 64 frames)."""
+    wb, cfg, frames, targets, theta0, target_theta = c5[:6]
+    pot = ElecLJ(precision="fp64", **cfg).init(wb)
+    theta, L, calls = fit_water(pot, wb.site_mask, frames[:8], targets[:8], theta0, maxiter=60)
+    pot.close()
+    assert np.abs(theta / target_theta - 1).max() < 1e-6, (theta, target_theta, L, calls)
