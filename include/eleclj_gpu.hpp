@@ -149,6 +149,48 @@ public:
     lj_correction = e.lj_correction;
   }
 
+  // add_to_energy_and_forces through mmnb_forward: the same energy and forces,
+  // and the site potentials and fields stay on the device for site_gradients
+  // (the forward pass of a parameter fit; the backward does not evaluate again)
+  void forward(double &u, Cartesian *f)
+  {
+    for (int i = 0; i < nsite; i++)
+      r[i] = site[i]->position(msys->atom);
+    fs.assign(3 * (size_t) nsite, 0.0);
+    mmnb_energy e;
+    if (mmnb_forward(h, (const double *) r, fs.data(), &u, &e) != MMNB_OK)
+      die("ElecLJGpu::forward: %s", mmnb_last_error(h));
+    for (int i = 0; i < nsite; i++)
+      site[i]->apply_force(msys->atom, f, Cartesian(fs[3 * i], fs[3 * i + 1], fs[3 * i + 2]));
+    elec_energy = e.elec;
+    lj_energy = e.lj;
+    lj_correction = e.lj_correction;
+  }
+
+  // mmnb_site_gradients for the last forward(): per site dU/dq (charge units),
+  // dU/dsigma, dU/depsilon and, given dL/dF per SITE (3*nsite, or 0; for sites
+  // that are atoms this is dL/dF of the atom), the same three for the loss L.
+  // Any output may be 0.
+  void site_gradients(const double *dl_df, double *du_dq, double *du_dsig, double *du_deps, double *dl_dq,
+                      double *dl_dsig, double *dl_deps)
+  {
+    if (mmnb_site_gradients(h, dl_df, du_dq, du_dsig, du_deps, dl_dq, dl_dsig, dl_deps) != MMNB_OK)
+      die("ElecLJGpu::site_gradients: %s", mmnb_last_error(h));
+  }
+
+  // the gradient with respect to one type's parameter, as types_changed maps
+  // fixed_charge, sigma and epsilon to the sites of that type
+  // (src/eleclj.cpp:440-503): the sum over the sites whose type1 is `type`;
+  // multiply a charge sum by e_to_charge_unit(1) for d/d(charge in e)
+  double type_sum(const char *type, const double *site_grad) const
+  {
+    double s = 0;
+    for (int i = 0; i < nsite; i++)
+      if (site[i]->type1 == Str(type))
+        s += site_grad[i];
+    return s;
+  }
+
   // ElecLJ::electrostatic_potential_at_gridpoints (src/eleclj.cpp:1302-1340),
   // periodic boxes: the potential at each grid point; p also holds the sites'
   // entries after the points, as the reference's does
