@@ -533,6 +533,254 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// The row group's own constants in the rigid-water kernels: H offsets and
+// charges, O charge and LJ parameters, the FP64 anchor, packed constants.
+struct WaterRow {
+  f2 h12x, h12y, h12z, h21x, h21y, h21z;
+  float qO, qH1, qH2;
+  float2 ljo;
+  float qO32, qH1_32, qH2_32;  // charges times the fixed-point scale
+  WaterConst2 c2;
+  ErfcConst2 ke;
+  double4 ai;
+};
+
+__device__ __forceinline__ WaterRow water_row_consts(const WaterArgs &a, int p)
+{
+  constexpr float kTwo32 = 4294967296.0f;
+  WaterRow w;
+  const float4 r0 = a.site[3 * (size_t) p], r1 = a.site[3 * (size_t) p + 1], r2 = a.site[3 * (size_t) p + 2];
+  w.ai = a.anchor[p];
+  w.h12x = f2_pack(r0.x, r0.y);
+  w.h12y = f2_pack(r0.z, r0.w);
+  w.h12z = f2_pack(r1.x, r1.y);
+  w.h21x = f2_pack(r0.y, r0.x);
+  w.h21y = f2_pack(r0.w, r0.z);
+  w.h21z = f2_pack(r1.y, r1.x);
+  w.qO = r2.x;
+  w.qH1 = r1.z;
+  w.qH2 = r1.w;
+  w.ljo = make_float2(r2.z, r2.w);
+  // the converted values come out of the last product directly
+  w.qO32 = w.qO * kTwo32;
+  w.qH1_32 = w.qH1 * kTwo32;
+  w.qH2_32 = w.qH2 * kTwo32;
+  w.c2.pe = f2_dup(a.pe);
+  w.c2.one = f2_dup(1.f);
+  w.c2.nel2 = f2_dup(a.nel2);
+  w.c2.c2 = f2_dup(a.c2);
+  w.ke.e[0] = f2_dup(kE0);
+  w.ke.e[1] = f2_dup(kE1);
+  w.ke.e[2] = f2_dup(kE2);
+  w.ke.e[3] = f2_dup(kE3);
+  w.ke.e[4] = f2_dup(kE4);
+  w.ke.e[5] = f2_dup(kE5);
+  w.ke.e[6] = f2_dup(kE6);
+  w.ke.e[7] = f2_dup(kE7);
+  return w;
+}
+
+// One group pair inside the cutoff: da = anchor displacement (xyz) and its
+// r^2, j0, j1, j2 = the partner's three packed slots.  Adds the row sites'
+// fixed-point force words, the pair energies and (VIR) the virial term to fx.
+template <bool VIR>
+__device__ __forceinline__ void water_pair(const WaterArgs &a, const WaterRow &w, float4 da, ulonglong2 j0,
+                                           ulonglong2 j1, float4 j2, long long (&fx)[VIR ? 12 : 11])
+{
+  constexpr float kTwo32 = 4294967296.0f, kTwo31 = 2147483648.0f;
+  const f2 jx = f2_of(j0.x), jy = f2_of(j0.y), jz = f2_of(j1.x), qj = f2_of(j1.y);
+  const float qjO = j2.x;
+  // switch S(z) and dS/dr^2 (zero inside rc - width), branch-free
+  const float z = fmaxf(da.w - a.rlo2, 0.f) * a.inv_sw;
+  const float zz = z * z;
+  const float s = fmaf(fmaf(fmaf(-6.f, z, 15.f), z, -10.f), zz * z, 1.f);
+  const float ds = fmaf(fmaf(60.f, z, -120.f), z, 60.f) * zz * a.inv_sw;
+  const f2 s2 = f2_dup(s);
+  const f2 qbs = mul2(qj, s2);
+  const f2 q0d = f2_pack(j2.x, j2.y);
+  const f2 q0s = mul2(q0d, s2);
+  const f2 dx = f2_dup(da.x), dy = f2_dup(da.y), dz = f2_dup(da.z);
+  // row O against partner O (single) and partner H1, H2 (packed)
+  float eOx = 0.f, eOy = 0.f, eOz = 0.f, tO = 0.f, rOO;
+  water_site(da.x, da.y, da.z, qjO, qjO * s, a, eOx, eOy, eOz, tO, rOO);
+  f2 aOx = f2_dup(0.f), aOy = aOx, aOz = aOx, aOt = aOx;
+  water_site2(sub2(dx, jx), sub2(dy, jy), sub2(dz, jz), qj, qbs, w.c2, w.ke, aOx, aOy, aOz, aOt);
+  // rows H1, H2 against partner O, then against partner H1, H2 in order
+  const f2 cx = add2(dx, w.h12x), cy = add2(dy, w.h12y), cz = add2(dz, w.h12z);
+  f2 hx = f2_dup(0.f), hy = hx, hz = hx, ht = hx;
+  water_site2(cx, cy, cz, q0d, q0s, w.c2, w.ke, hx, hy, hz, ht);
+  water_site2(sub2(cx, jx), sub2(cy, jy), sub2(cz, jz), qj, qbs, w.c2, w.ke, hx, hy, hz, ht);
+  // rows H2, H1 against partner H1, H2
+  f2 vx = f2_dup(0.f), vy = vx, vz = vx, vt = vx;
+  water_site2(sub2(add2(dx, w.h21x), jx), sub2(add2(dy, w.h21y), jy), sub2(add2(dz, w.h21z), jz), qj, qbs, w.c2,
+              w.ke, vx, vy, vz, vt);
+  eOx += f2_lo(aOx) + f2_hi(aOx);
+  eOy += f2_lo(aOy) + f2_hi(aOy);
+  eOz += f2_lo(aOz) + f2_hi(aOz);
+  tO += f2_lo(aOt) + f2_hi(aOt);
+  const float e1x = f2_lo(hx) + f2_hi(vx), e1y = f2_lo(hy) + f2_hi(vy), e1z = f2_lo(hz) + f2_hi(vz);
+  const float e2x = f2_hi(hx) + f2_lo(vx), e2y = f2_hi(hy) + f2_lo(vy), e2z = f2_hi(hz) + f2_lo(vz);
+  const float t1 = f2_lo(ht) + f2_hi(vt), t2 = f2_hi(ht) + f2_lo(vt);
+  // O-O Lennard-Jones
+  const float sj = j2.z, ej = j2.w;
+  const float sg = a.geometric ? w.ljo.x * sj : 0.5f * (w.ljo.x + sj);
+  const float sq = a.geometric ? sg : sg * sg;
+  const float s6 = sq * sq * sq;
+  const float b = 4.f * w.ljo.y * ej * s6;
+  const float ir2 = rOO * rOO;
+  const float ir6 = ir2 * ir2 * ir2;
+  const float bi6 = b * ir6;
+  const float ai12 = b * s6 * ir6 * ir6;
+  const float u = ai12 - bi6;
+  const float du = (12.f * ai12 - 6.f * bi6) * ir2 * s;
+  // unswitched Coulomb energy of the group pair; its switched half is the
+  // row's energy share and, with u, it scales the switch derivative
+  const float tq = fmaf(w.qO, tO, fmaf(w.qH1, t1, w.qH2 * t2));
+  const float g = ds * (tq + u);
+  const float fo32 = (du + g) * kTwo32;
+  const float s31 = s * kTwo31;
+  fx[0] += __float2ll_rn(fmaf(w.qO32, eOx, fo32 * da.x));
+  fx[1] += __float2ll_rn(fmaf(w.qO32, eOy, fo32 * da.y));
+  fx[2] += __float2ll_rn(fmaf(w.qO32, eOz, fo32 * da.z));
+  fx[3] += __float2ll_rn(w.qH1_32 * e1x);
+  fx[4] += __float2ll_rn(w.qH1_32 * e1y);
+  fx[5] += __float2ll_rn(w.qH1_32 * e1z);
+  fx[6] += __float2ll_rn(w.qH2_32 * e2x);
+  fx[7] += __float2ll_rn(w.qH2_32 * e2y);
+  fx[8] += __float2ll_rn(w.qH2_32 * e2z);
+  fx[9] += __float2ll_rn(tq * s31);
+  fx[10] += __float2ll_rn(u * s31);
+  if constexpr (VIR)
+    fx[11] += __float2ll_rn(0.5f * fo32 * da.w);  // each pair is seen from both rows
+}
+
+// One row group p, partners queued through the warp's ring: walks the row's
+// list (full rows, making the pruned ones, or the pruned rows); each lane
+// tests one partner's anchor distance, an accepted partner's displacement goes
+// to the ring and its record is copied there (cp.async); 32 queued pairs are
+// evaluated at a time, one per lane.  qa, q0, q1, q2: the warp's ring.
+// Returns the row's first site.
+template <bool VIR>
+__device__ __forceinline__ int water_row(const WaterArgs &a, int p, int lane, float4 *qa, float4 *q0, float4 *q1,
+                                         float4 *q2, long long (&fx)[VIR ? 12 : 11])
+{
+  constexpr int kMask = kWaterRing - 1;
+  const WaterRow w = water_row_consts(a, p);
+  const double4 ai = w.ai;
+  const int si0 = a.group[2 * a.sorted[p]];
+  // full rows (and make the pruned ones), or the pruned rows
+  const bool make = a.pnbr && a.flags[kFlagPruneFull];
+  const bool use_pruned = a.pnbr && !make;
+  const int cnt = use_pruned ? a.pcount[p] : a.nbr_count[p];
+  const int *row = (use_pruned ? a.pnbr : a.nbr) + (size_t) p * a.rowcap;
+  int *prow = make ? a.pnbr + (size_t) p * a.rowcap : nullptr;
+  int pn = 0;
+  const unsigned below = (1u << lane) - 1;
+  auto compute = [&](int k) {
+    water_pair<VIR>(a, w, qa[k], *reinterpret_cast<const ulonglong2 *>(&q0[k]),
+                    *reinterpret_cast<const ulonglong2 *>(&q1[k]), q2[k], fx);
+  };
+  // Entries past the row end read the row's own group (a valid address);
+  // they are never accepted.
+  int jc = lane < cnt ? row[lane] : p;
+  int jn = lane + 32 < cnt ? row[lane + 32] : p;
+  double4 ac = a.anchor[jc];
+  int head = 0, qn = 0;  // ring entries [head, head + qn)
+  for (int base = 0; base < cnt; base += 32) {
+    const int e2 = base + 64 + lane;
+    const int jnn = e2 < cnt ? row[e2] : p;
+    const double4 an = a.anchor[jn];
+    double x, y, z;
+    const double r2a = anchor_disp_fast(a.box, ai, ac, x, y, z);
+    const bool take = base + lane < cnt && r2a <= a.rhi2;
+    if (make) {
+      const bool keep = base + lane < cnt && r2a <= a.rp2;
+      const unsigned kb = __ballot_sync(0xffffffffu, keep);
+      if (keep)
+        prow[pn + __popc(kb & below)] = jc;
+      pn += __popc(kb);
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, take);
+    if (take) {
+      const int slot = (head + qn + __popc(bal & below)) & kMask;
+      qa[slot] = make_float4((float) x, (float) y, (float) z, (float) r2a);
+      const float4 *src = a.site + 3 * (size_t) jc;
+      cp_async16(&q0[slot], src);
+      cp_async16(&q1[slot], src + 1);
+      cp_async16(&q2[slot], src + 2);
+    }
+    cp_async_commit();
+    // entries of earlier batches are evaluated one batch after their copies
+    // were started, so the copies are normally complete by then
+    const bool run = qn >= 32;
+    qn += __popc(bal);
+    if (run) {
+      cp_async_wait_prev();
+      __syncwarp();
+      compute((head + lane) & kMask);
+      __syncwarp();  // the slots are free again only after every lane has read them
+      head = (head + 32) & kMask;
+      qn -= 32;
+    }
+    jc = jn;
+    jn = jnn;
+    ac = an;
+  }
+  cp_async_wait_all();
+  __syncwarp();
+  for (; qn > 0; qn -= 32, head = (head + 32) & kMask)
+    if (lane < qn)
+      compute((head + lane) & kMask);
+  if (make && lane == 0) {
+    a.pcount[p] = pn;
+    a.plast[3 * p] = ai.x;
+    a.plast[3 * p + 1] = ai.y;
+    a.plast[3 * p + 2] = ai.z;
+  }
+  return si0;
+}
+
+// The lanes' fixed-point totals of a finished row by a butterfly
+// reduce-scatter over the warp (no shared memory): the 16 columns (the totals,
+// padded) halve at each of four exchange steps, each lane keeping the half
+// its lane bit selects, and a last exchange completes the sum, so the lane
+// pair (2c, 2c+1) holds the total of column c.  Integer sums: the same bits as
+// any other order.  The nine force words go to acc, the potential and field
+// words of the three sites are cleared (P3M adds to them), and every lane gets
+// the row's Coulomb and LJ pair energies and virial term.
+template <bool VIR>
+__device__ __forceinline__ void water_row_store_shfl(const WaterArgs &a, int si0, int lane,
+                                                     const long long (&fx)[VIR ? 12 : 11], long long &te,
+                                                     long long &tl, long long &tv)
+{
+  constexpr int kCols = VIR ? 12 : 11;
+  long long v[16];
+#pragma unroll
+  for (int c = 0; c < 16; c++)
+    v[c] = c < kCols ? fx[c] : 0;
+#pragma unroll
+  for (int half = 8; half >= 1; half >>= 1) {
+    const bool up = lane & (2 * half);
+#pragma unroll
+    for (int k = 0; k < half; k++) {
+      const long long keep = up ? v[k + half] : v[k];
+      const long long send = up ? v[k] : v[k + half];
+      v[k] = keep + __shfl_xor_sync(0xffffffffu, send, 2 * half);
+    }
+  }
+  const long long t = v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+  const int c = (lane >> 1) & 15;
+  if (!(lane & 1)) {
+    if (c < 9)
+      a.acc[(size_t) (si0 + c / 3) * kAccStride + 4 + c % 3] = t;
+  } else if (c < 12) {
+    a.acc[(size_t) (si0 + c / 4) * kAccStride + c % 4] = 0;
+  }
+  te = __shfl_sync(0xffffffffu, t, 2 * 9);
+  tl = __shfl_sync(0xffffffffu, t, 2 * 10);
+  tv = VIR ? __shfl_sync(0xffffffffu, t, 2 * 11) : 0;
+}
+
 // MINB: resident warps per SM / 4 the register budget is cut for (4: 128
 // registers, 5: 96); mmnb_autotune picks per handle
 // VIR: also the part of dU/ds (box scaling) the site forces do not carry, the
@@ -543,213 +791,32 @@ __global__ void __launch_bounds__(kWaterWarps * 32, MINB * kMxWarps / kWaterWarp
   // per warp: ring of anchor displacement (xyz, r^2) and the partner's three
   // packed slots
   __shared__ float4 ring[kWaterWarps][4][kWaterRing];
+  __shared__ long long wsum[kWaterWarps][3];
   constexpr int kCols = VIR ? 12 : 11;
-  constexpr int kMask = kWaterRing - 1;
-  constexpr float kTwo32 = 4294967296.0f, kTwo31 = 2147483648.0f;
-  long long fx[kCols];
-#pragma unroll
-  for (int c = 0; c < kCols; c++)
-    fx[c] = 0;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int p = blockIdx.x * kWaterWarps + w;
-  float4 *qa = ring[w][0], *q0 = ring[w][1], *q1 = ring[w][2], *q2 = ring[w][3];
-  int si0 = 0;
+  long long te = 0, tl = 0, tv = 0;
   if (p < a.ngroup) {
-    // the row's own record: H offsets and charges, O charge and LJ parameters
-    const float4 r0 = a.site[3 * (size_t) p], r1 = a.site[3 * (size_t) p + 1], r2 = a.site[3 * (size_t) p + 2];
-    const double4 ai = a.anchor[p];
-    const f2 h12x = f2_pack(r0.x, r0.y), h12y = f2_pack(r0.z, r0.w), h12z = f2_pack(r1.x, r1.y);
-    const f2 h21x = f2_pack(r0.y, r0.x), h21y = f2_pack(r0.w, r0.z), h21z = f2_pack(r1.y, r1.x);
-    const float qO = r2.x, qH1 = r1.z, qH2 = r1.w;
-    const float2 ljo = make_float2(r2.z, r2.w);
-    // charges times the fixed-point scale: the converted values come out of
-    // the last product directly
-    const float qO32 = qO * kTwo32, qH1_32 = qH1 * kTwo32, qH2_32 = qH2 * kTwo32;
-    WaterConst2 c2;
-    c2.pe = f2_dup(a.pe);
-    c2.one = f2_dup(1.f);
-    c2.nel2 = f2_dup(a.nel2);
-    c2.c2 = f2_dup(a.c2);
-    ErfcConst2 ke;
-    ke.e[0] = f2_dup(kE0);
-    ke.e[1] = f2_dup(kE1);
-    ke.e[2] = f2_dup(kE2);
-    ke.e[3] = f2_dup(kE3);
-    ke.e[4] = f2_dup(kE4);
-    ke.e[5] = f2_dup(kE5);
-    ke.e[6] = f2_dup(kE6);
-    ke.e[7] = f2_dup(kE7);
-    si0 = a.group[2 * a.sorted[p]];
-    // full rows (and make the pruned ones), or the pruned rows
-    const bool make = a.pnbr && a.flags[kFlagPruneFull];
-    const bool use_pruned = a.pnbr && !make;
-    const int cnt = use_pruned ? a.pcount[p] : a.nbr_count[p];
-    const int *row = (use_pruned ? a.pnbr : a.nbr) + (size_t) p * a.rowcap;
-    int *prow = make ? a.pnbr + (size_t) p * a.rowcap : nullptr;
-    int pn = 0;
-    const unsigned below = (1u << lane) - 1;
-    auto compute = [&](int k) {
-      const float4 da = qa[k];
-      const ulonglong2 j0 = *reinterpret_cast<const ulonglong2 *>(&q0[k]);
-      const ulonglong2 j1 = *reinterpret_cast<const ulonglong2 *>(&q1[k]);
-      const float4 j2 = q2[k];
-      const f2 jx = f2_of(j0.x), jy = f2_of(j0.y), jz = f2_of(j1.x), qj = f2_of(j1.y);
-      const float qjO = j2.x;
-      // switch S(z) and dS/dr^2 (zero inside rc - width), branch-free
-      const float z = fmaxf(da.w - a.rlo2, 0.f) * a.inv_sw;
-      const float zz = z * z;
-      const float s = fmaf(fmaf(fmaf(-6.f, z, 15.f), z, -10.f), zz * z, 1.f);
-      const float ds = fmaf(fmaf(60.f, z, -120.f), z, 60.f) * zz * a.inv_sw;
-      const f2 s2 = f2_dup(s);
-      const f2 qbs = mul2(qj, s2);
-      const f2 q0d = f2_pack(j2.x, j2.y);
-      const f2 q0s = mul2(q0d, s2);
-      const f2 dx = f2_dup(da.x), dy = f2_dup(da.y), dz = f2_dup(da.z);
-      // row O against partner O (single) and partner H1, H2 (packed)
-      float eOx = 0.f, eOy = 0.f, eOz = 0.f, tO = 0.f, rOO;
-      water_site(da.x, da.y, da.z, qjO, qjO * s, a, eOx, eOy, eOz, tO, rOO);
-      f2 aOx = f2_dup(0.f), aOy = aOx, aOz = aOx, aOt = aOx;
-      water_site2(sub2(dx, jx), sub2(dy, jy), sub2(dz, jz), qj, qbs, c2, ke, aOx, aOy, aOz, aOt);
-      // rows H1, H2 against partner O, then against partner H1, H2 in order
-      const f2 cx = add2(dx, h12x), cy = add2(dy, h12y), cz = add2(dz, h12z);
-      f2 hx = f2_dup(0.f), hy = hx, hz = hx, ht = hx;
-      water_site2(cx, cy, cz, q0d, q0s, c2, ke, hx, hy, hz, ht);
-      water_site2(sub2(cx, jx), sub2(cy, jy), sub2(cz, jz), qj, qbs, c2, ke, hx, hy, hz, ht);
-      // rows H2, H1 against partner H1, H2
-      f2 wx = f2_dup(0.f), wy = wx, wz = wx, wt = wx;
-      water_site2(sub2(add2(dx, h21x), jx), sub2(add2(dy, h21y), jy), sub2(add2(dz, h21z), jz), qj, qbs, c2, ke,
-                  wx, wy, wz, wt);
-      eOx += f2_lo(aOx) + f2_hi(aOx);
-      eOy += f2_lo(aOy) + f2_hi(aOy);
-      eOz += f2_lo(aOz) + f2_hi(aOz);
-      tO += f2_lo(aOt) + f2_hi(aOt);
-      const float e1x = f2_lo(hx) + f2_hi(wx), e1y = f2_lo(hy) + f2_hi(wy), e1z = f2_lo(hz) + f2_hi(wz);
-      const float e2x = f2_hi(hx) + f2_lo(wx), e2y = f2_hi(hy) + f2_lo(wy), e2z = f2_hi(hz) + f2_lo(wz);
-      const float t1 = f2_lo(ht) + f2_hi(wt), t2 = f2_hi(ht) + f2_lo(wt);
-      // O-O Lennard-Jones
-      const float sj = j2.z, ej = j2.w;
-      const float sg = a.geometric ? ljo.x * sj : 0.5f * (ljo.x + sj);
-      const float sq = a.geometric ? sg : sg * sg;
-      const float s6 = sq * sq * sq;
-      const float b = 4.f * ljo.y * ej * s6;
-      const float ir2 = rOO * rOO;
-      const float ir6 = ir2 * ir2 * ir2;
-      const float bi6 = b * ir6;
-      const float ai12 = b * s6 * ir6 * ir6;
-      const float u = ai12 - bi6;
-      const float du = (12.f * ai12 - 6.f * bi6) * ir2 * s;
-      // unswitched Coulomb energy of the group pair; its switched half is the
-      // row's energy share and, with u, it scales the switch derivative
-      const float tq = fmaf(qO, tO, fmaf(qH1, t1, qH2 * t2));
-      const float g = ds * (tq + u);
-      const float fo32 = (du + g) * kTwo32;
-      const float s31 = s * kTwo31;
-      fx[0] += __float2ll_rn(fmaf(qO32, eOx, fo32 * da.x));
-      fx[1] += __float2ll_rn(fmaf(qO32, eOy, fo32 * da.y));
-      fx[2] += __float2ll_rn(fmaf(qO32, eOz, fo32 * da.z));
-      fx[3] += __float2ll_rn(qH1_32 * e1x);
-      fx[4] += __float2ll_rn(qH1_32 * e1y);
-      fx[5] += __float2ll_rn(qH1_32 * e1z);
-      fx[6] += __float2ll_rn(qH2_32 * e2x);
-      fx[7] += __float2ll_rn(qH2_32 * e2y);
-      fx[8] += __float2ll_rn(qH2_32 * e2z);
-      fx[9] += __float2ll_rn(tq * s31);
-      fx[10] += __float2ll_rn(u * s31);
-      if constexpr (VIR)
-        fx[11] += __float2ll_rn(0.5f * fo32 * da.w);  // each pair is seen from both rows
-    };
-    // Entries past the row end read the row's own group (a valid address);
-    // they are never accepted.
-    int jc = lane < cnt ? row[lane] : p;
-    int jn = lane + 32 < cnt ? row[lane + 32] : p;
-    double4 ac = a.anchor[jc];
-    int head = 0, qn = 0;  // ring entries [head, head + qn)
-    for (int base = 0; base < cnt; base += 32) {
-      const int e2 = base + 64 + lane;
-      const int jnn = e2 < cnt ? row[e2] : p;
-      const double4 an = a.anchor[jn];
-      double x, y, z;
-      const double r2a = anchor_disp_fast(a.box, ai, ac, x, y, z);
-      const bool take = base + lane < cnt && r2a <= a.rhi2;
-      if (make) {
-        const bool keep = base + lane < cnt && r2a <= a.rp2;
-        const unsigned kb = __ballot_sync(0xffffffffu, keep);
-        if (keep)
-          prow[pn + __popc(kb & below)] = jc;
-        pn += __popc(kb);
-      }
-      const unsigned bal = __ballot_sync(0xffffffffu, take);
-      if (take) {
-        const int slot = (head + qn + __popc(bal & below)) & kMask;
-        qa[slot] = make_float4((float) x, (float) y, (float) z, (float) r2a);
-        const float4 *src = a.site + 3 * (size_t) jc;
-        cp_async16(&q0[slot], src);
-        cp_async16(&q1[slot], src + 1);
-        cp_async16(&q2[slot], src + 2);
-      }
-      cp_async_commit();
-      // entries of earlier batches are evaluated one batch after their copies
-      // were started, so the copies are normally complete by then
-      const bool run = qn >= 32;
-      qn += __popc(bal);
-      if (run) {
-        cp_async_wait_prev();
-        __syncwarp();
-        compute((head + lane) & kMask);
-        __syncwarp();  // the slots are free again only after every lane has read them
-        head = (head + 32) & kMask;
-        qn -= 32;
-      }
-      jc = jn;
-      jn = jnn;
-      ac = an;
-    }
-    cp_async_wait_all();
-    __syncwarp();
-    for (; qn > 0; qn -= 32, head = (head + 32) & kMask)
-      if (lane < qn)
-        compute((head + lane) & kMask);
-    if (make && lane == 0) {
-      a.pcount[p] = pn;
-      a.plast[3 * p] = ai.x;
-      a.plast[3 * p + 1] = ai.y;
-      a.plast[3 * p + 2] = ai.z;
-    }
+    long long fx[kCols];
+#pragma unroll
+    for (int c = 0; c < kCols; c++)
+      fx[c] = 0;
+    const int si0 = water_row<VIR>(a, p, lane, ring[w][0], ring[w][1], ring[w][2], ring[w][3], fx);
+    water_row_store_shfl<VIR>(a, si0, lane, fx, te, tl, tv);
   }
   if (a.pnbr && a.flags[kFlagPruneFull] && blockIdx.x == 0 && threadIdx.x == 0)
     a.flags[kFlagPruneValid] = 1;
-  __shared__ long long wsum[kWaterWarps][3];
-  // lane totals, transposed through the warp's own ring (no longer in use)
-  static_assert(32 * (kCols + 1) * sizeof(long long) <= sizeof(ring[0]), "ring too small for the reduction");
-  long long(*red)[kCols + 1] = reinterpret_cast<long long(*)[kCols + 1]>(ring[w]);
-  __syncwarp();
-#pragma unroll
-  for (int c = 0; c < kCols; c++)
-    red[lane][c] = fx[c];
-  __syncwarp();
-  if (lane < kCols) {
-    long long t = 0;
-    for (int l = 0; l < 32; l++)
-      t += red[l][lane];
-    if (lane < 9) {
-      if (p < a.ngroup)
-        a.acc[(size_t) (si0 + lane / 3) * kAccStride + 4 + lane % 3] = t;
-    } else {
-      wsum[w][lane - 9] = t;
-    }
-  } else if (lane < kCols + 12 && p < a.ngroup) {
-    // clear the potential and field slots of the three sites (P3M adds to them)
-    const int k = lane - kCols;
-    a.acc[(size_t) (si0 + k / 4) * kAccStride + k % 4] = 0;
+  if (lane == 0) {
+    wsum[w][0] = te;
+    wsum[w][1] = tl;
+    wsum[w][2] = tv;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    long long te = 0, tl = 0, tv = 0;
-    for (int k = 0; k < kWaterWarps; k++) {
+    for (int k = 1; k < kWaterWarps; k++) {
       te += wsum[k][0];
       tl += wsum[k][1];
-      if (VIR)
-        tv += wsum[k][2];
+      tv += wsum[k][2];
     }
     // integer sums: the totals do not depend on the order blocks finish in
     atomicAdd(a.wsum, (unsigned long long) te);
@@ -785,6 +852,7 @@ cudaError_t launch_rspace_water(mmnb_handle *h)
   a.plast = h->d_plast;
   a.flags = h->d_flags;
   a.rp2 = (h->rc + h->prune_margin) * (h->rc + h->prune_margin);
+  h->launches += 1;
   const int blocks = div_up(h->ngroup, kWaterWarps);
   if (h->want_virial)
     k_pair_water<4, true><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
@@ -792,7 +860,6 @@ cudaError_t launch_rspace_water(mmnb_handle *h)
     k_pair_water<5, false><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
   else
     k_pair_water<4, false><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
-  h->launches += 1;
   return cudaGetLastError();
 }
 
