@@ -438,7 +438,7 @@ void free_all(mmnb_handle *h)
                   h->d_phi, h->d_evec, h->d_ljf, h->d_lj_part, h->d_elec_part, h->d_energy, h->d_r, h->d_f,
                   h->d_mesh, h->d_meshk, h->d_green, h->d_kvec, h->d_egrid, h->d_egridk, h->d_mesh32,
                   h->d_meshk32, h->d_green32, h->d_mesh_fx, h->d_kint, h->d_kvecs, h->d_ak, h->d_skc,
-                  h->mx.site, h->mx.par, h->mx.anchor, h->mx.acc, h->mx.acck, h->d_wsum,
+                  h->mx.site, h->mx.par, h->mx.anchor, h->mx.anc32, h->mx.acc, h->mx.acck, h->d_wsum,
                   h->d_bwd, h->d_gmesh, h->d_gmeshk};
   for (void *p : ptrs)
     if (p)
@@ -735,7 +735,7 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
   CK(cudaMemset(h->d_wsum, 0, sizeof(unsigned long long) * 8));
   if (c->precision == MMNB_MIXED) {
     if ((s = dalloc(h, &h->mx.site, nslot)) || (s = dalloc(h, &h->mx.par, nslot)) ||
-        (s = dalloc(h, &h->mx.anchor, ngroup)) ||
+        (s = dalloc(h, &h->mx.anchor, ngroup)) || (s = dalloc(h, &h->mx.anc32, ngroup)) ||
         (s = dalloc(h, &h->mx.acc, (size_t) nsite * kAccStride)) ||
         (s = dalloc(h, &h->mx.acck, (size_t) nsite * 4)))
       return s;
@@ -878,6 +878,19 @@ int mmnb_set_params(mmnb_handle *h, const int *site_mask, const double *q, const
     const int a = h->group[2 * g];
     h->water = h->group[2 * g + 1] - a == 3 && site_mask[a] == (MMNB_SITE_HAS_Q | MMNB_SITE_HAS_LJ) &&
                site_mask[a + 1] == MMNB_SITE_HAS_Q && site_mask[a + 2] == MMNB_SITE_HAS_Q;
+  }
+  h->water_uni = h->water && h->ngroup > 0;
+  if (h->water_uni) {
+    const int a = h->group[0];
+    for (int g = 0; g < h->ngroup && h->water_uni; g++) {
+      const int b = h->group[2 * g];
+      h->water_uni = q[b] == q[a] && sig[b] == sig[a] && eps[b] == eps[a] && q[b + 1] == q[a + 1] &&
+                     q[b + 2] == q[a + 1];
+    }
+    h->uni_qO = (float) q[a];
+    h->uni_qH = (float) q[a + 1];
+    h->uni_sig = (float) sig[a];
+    h->uni_seps = (float) sqrt(eps[a]);
   }
   h->params_set = true;
   return MMNB_OK;

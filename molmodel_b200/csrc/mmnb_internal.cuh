@@ -65,6 +65,8 @@ struct MixedBufs {
                                  // for the rigid-water kernel, three packed slots per group
   float4 *par = nullptr;         // sorted, padded slots: sigma, sqrt(epsilon), rscreen, mask bits
   double4 *anchor = nullptr;     // sorted groups: anchor position (FP64)
+  float4 *anc32 = nullptr;       // rigid-water kernel, sorted groups: the anchor's offset from the corner
+                                 // of its list cell (FP32) and the cell's coordinates (10 bits each, in w)
   long long *acc = nullptr;      // per site (original order), kAccStride fixed-point values
   long long *acck = nullptr;     // per site (original order): P3M interpolation phi, Ex, Ey, Ez
 };
@@ -101,6 +103,10 @@ struct mmnb_handle {
   bool any_gexcl = false, use_14 = false;
   bool lj_on_anchors_only = false;   // every LJ site is its group's first site (rigid water)
   bool water = false;                // every group is [O(q, LJ), H(q), H(q)] with no screening or group exclusions
+  // ... and every O has the same charge, sigma and epsilon and every H the
+  // same charge (the rigid-water kernel then copies only the H offsets)
+  bool water_uni = false;
+  float uni_qO = 0, uni_qH = 0, uni_sig = 0, uni_seps = 0;
   bool want_fields = false;          // this evaluation must produce per-site potential and field
   bool want_virial = false;          // this evaluation's pair kernels also sum the virial's pair term
   bool used_water = false;           // the last evaluation ran the water kernel

@@ -380,7 +380,13 @@ struct WaterArgs {
   double rhi2;
   float rlo2, inv_sw, pe, c2, nel2;  // pe = p eta (erfc argument scale)
   const float4 *site;     // 3 packed slots per sorted group (above)
-  const double4 *anchor;
+  const double4 *anchor;  // FP64 anchors (sorted groups): the prune bookkeeping
+  const float4 *anc32;    // cell-relative FP32 anchors (sorted groups, k_prep_mixed)
+  int ncell, nhalf;       // list cells per dimension, ncell / 2
+  float edge[3];          // cell edge, FP32 (the value the offsets were formed with)
+  float Lf[3], halfL[3];  // box edges and half edges, FP32
+  float rhi2f, rp2f;      // rc^2 and (rc + prune margin)^2, FP32
+  float uqO, uqH, usig, useps;  // uniform water: O and H charges, O sigma and sqrt(epsilon)
   const int *nbr, *nbr_count, *sorted, *group;
   long long *acc;         // per site: slots 4..6 receive the force, 0..3 are cleared
   unsigned long long *wsum;  // fixed-point Coulomb and LJ pair energies and, with the virial,
@@ -529,9 +535,47 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src)
                : "memory");
 }
 
+__device__ __forceinline__ void cp_async8(void *dst, const void *src)
+{
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned) __cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Anchor displacement (row minus partner) from the cell-relative FP32 anchors:
+// the integer cell difference wrapped to [-n/2, n/2] (exact), times the cell
+// edge, plus the offset difference, and one FP32 minimum-image correction,
+// which only pairs near half the box reach.  The offsets and the cell edge
+// are below ~5 A, so the result is within ~1e-6 A of the exact minimum-image
+// displacement for every pair a row can list (the FP64 form tests the cutoff
+// on the reference's rounding; here, as in the other mixed kernels, the pair
+// set may differ from it only by pairs at the cutoff, where the switch and its
+// derivative vanish).
+__device__ __forceinline__ float3 cell_disp(const WaterArgs &a, float4 ai, float4 aj)
+{
+  const int ci = __float_as_int(ai.w), cj = __float_as_int(aj.w);
+  const int dc[3] = {(ci & 1023) - (cj & 1023), ((ci >> 10) & 1023) - ((cj >> 10) & 1023),
+                     ((ci >> 20) & 1023) - ((cj >> 20) & 1023)};
+  const float dof[3] = {ai.x - aj.x, ai.y - aj.y, ai.z - aj.z};
+  float v[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    int d = dc[k];
+    d -= d > a.nhalf ? a.ncell : 0;
+    d += d < -a.nhalf ? a.ncell : 0;
+    // float(d) without a conversion instruction: 1.5 * 2^23 + d is exact
+    const float df = __int_as_float(d + 0x4B400000) - 12582912.0f;
+    float x = fmaf(df, a.edge[k], dof[k]);
+    x -= x > a.halfL[k] ? a.Lf[k] : 0.f;
+    x += x < -a.halfL[k] ? a.Lf[k] : 0.f;
+    v[k] = x;
+  }
+  return make_float3(v[0], v[1], v[2]);
+}
 
 // The row group's own constants in the rigid-water kernels: H offsets and
 // charges, O charge and LJ parameters, the FP64 anchor, packed constants.
@@ -542,15 +586,18 @@ struct WaterRow {
   float qO32, qH1_32, qH2_32;  // charges times the fixed-point scale
   WaterConst2 c2;
   ErfcConst2 ke;
-  double4 ai;
+  float4 ai;  // cell-relative FP32 anchor
 };
 
+// UNI: every water has the same parameters (taken from the arguments)
+template <bool UNI>
 __device__ __forceinline__ WaterRow water_row_consts(const WaterArgs &a, int p)
 {
   constexpr float kTwo32 = 4294967296.0f;
   WaterRow w;
-  const float4 r0 = a.site[3 * (size_t) p], r1 = a.site[3 * (size_t) p + 1], r2 = a.site[3 * (size_t) p + 2];
-  w.ai = a.anchor[p];
+  const float4 r0 = a.site[3 * (size_t) p], r1 = a.site[3 * (size_t) p + 1];
+  const float4 r2 = UNI ? make_float4(a.uqO, a.uqO, a.usig, a.useps) : a.site[3 * (size_t) p + 2];
+  w.ai = a.anc32[p];
   w.h12x = f2_pack(r0.x, r0.y);
   w.h12y = f2_pack(r0.z, r0.w);
   w.h12z = f2_pack(r1.x, r1.y);
@@ -558,8 +605,8 @@ __device__ __forceinline__ WaterRow water_row_consts(const WaterArgs &a, int p)
   w.h21y = f2_pack(r0.w, r0.z);
   w.h21z = f2_pack(r1.y, r1.x);
   w.qO = r2.x;
-  w.qH1 = r1.z;
-  w.qH2 = r1.w;
+  w.qH1 = UNI ? a.uqH : r1.z;
+  w.qH2 = UNI ? a.uqH : r1.w;
   w.ljo = make_float2(r2.z, r2.w);
   // the converted values come out of the last product directly
   w.qO32 = w.qO * kTwo32;
@@ -583,12 +630,16 @@ __device__ __forceinline__ WaterRow water_row_consts(const WaterArgs &a, int p)
 // One group pair inside the cutoff: da = anchor displacement (xyz) and its
 // r^2, j0, j1, j2 = the partner's three packed slots.  Adds the row sites'
 // fixed-point force words, the pair energies and (VIR) the virial term to fx.
-template <bool VIR>
+// With UNI the partner's charges and LJ parameters are the arguments' and
+// only j0 and the first half of j1 (the H offsets) are read.
+template <bool VIR, bool UNI>
 __device__ __forceinline__ void water_pair(const WaterArgs &a, const WaterRow &w, float4 da, ulonglong2 j0,
                                            ulonglong2 j1, float4 j2, long long (&fx)[VIR ? 12 : 11])
 {
   constexpr float kTwo32 = 4294967296.0f, kTwo31 = 2147483648.0f;
-  const f2 jx = f2_of(j0.x), jy = f2_of(j0.y), jz = f2_of(j1.x), qj = f2_of(j1.y);
+  if (UNI)
+    j2 = make_float4(a.uqO, a.uqO, a.usig, a.useps);
+  const f2 jx = f2_of(j0.x), jy = f2_of(j0.y), jz = f2_of(j1.x), qj = UNI ? f2_dup(a.uqH) : f2_of(j1.y);
   const float qjO = j2.x;
   // switch S(z) and dS/dr^2 (zero inside rc - width), branch-free
   const float z = fmaxf(da.w - a.rlo2, 0.f) * a.inv_sw;
@@ -660,13 +711,12 @@ __device__ __forceinline__ void water_pair(const WaterArgs &a, const WaterRow &w
 // to the ring and its record is copied there (cp.async); 32 queued pairs are
 // evaluated at a time, one per lane.  qa, q0, q1, q2: the warp's ring.
 // Returns the row's first site.
-template <bool VIR>
+template <bool VIR, bool UNI>
 __device__ __forceinline__ int water_row(const WaterArgs &a, int p, int lane, float4 *qa, float4 *q0, float4 *q1,
                                          float4 *q2, long long (&fx)[VIR ? 12 : 11])
 {
   constexpr int kMask = kWaterRing - 1;
-  const WaterRow w = water_row_consts(a, p);
-  const double4 ai = w.ai;
+  const WaterRow w = water_row_consts<UNI>(a, p);
   const int si0 = a.group[2 * a.sorted[p]];
   // full rows (and make the pruned ones), or the pruned rows
   const bool make = a.pnbr && a.flags[kFlagPruneFull];
@@ -677,24 +727,25 @@ __device__ __forceinline__ int water_row(const WaterArgs &a, int p, int lane, fl
   int pn = 0;
   const unsigned below = (1u << lane) - 1;
   auto compute = [&](int k) {
-    water_pair<VIR>(a, w, qa[k], *reinterpret_cast<const ulonglong2 *>(&q0[k]),
-                    *reinterpret_cast<const ulonglong2 *>(&q1[k]), q2[k], fx);
+    water_pair<VIR, UNI>(a, w, qa[k], *reinterpret_cast<const ulonglong2 *>(&q0[k]),
+                         *reinterpret_cast<const ulonglong2 *>(&q1[k]), UNI ? make_float4(0.f, 0.f, 0.f, 0.f) : q2[k],
+                         fx);
   };
   // Entries past the row end read the row's own group (a valid address);
   // they are never accepted.
   int jc = lane < cnt ? row[lane] : p;
   int jn = lane + 32 < cnt ? row[lane + 32] : p;
-  double4 ac = a.anchor[jc];
+  float4 ac = a.anc32[jc];
   int head = 0, qn = 0;  // ring entries [head, head + qn)
   for (int base = 0; base < cnt; base += 32) {
     const int e2 = base + 64 + lane;
     const int jnn = e2 < cnt ? row[e2] : p;
-    const double4 an = a.anchor[jn];
-    double x, y, z;
-    const double r2a = anchor_disp_fast(a.box, ai, ac, x, y, z);
-    const bool take = base + lane < cnt && r2a <= a.rhi2;
+    const float4 an = a.anc32[jn];
+    const float3 d = cell_disp(a, w.ai, ac);
+    const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
+    const bool take = base + lane < cnt && r2 <= a.rhi2f;
     if (make) {
-      const bool keep = base + lane < cnt && r2a <= a.rp2;
+      const bool keep = base + lane < cnt && r2 <= a.rp2f;
       const unsigned kb = __ballot_sync(0xffffffffu, keep);
       if (keep)
         prow[pn + __popc(kb & below)] = jc;
@@ -703,11 +754,15 @@ __device__ __forceinline__ int water_row(const WaterArgs &a, int p, int lane, fl
     const unsigned bal = __ballot_sync(0xffffffffu, take);
     if (take) {
       const int slot = (head + qn + __popc(bal & below)) & kMask;
-      qa[slot] = make_float4((float) x, (float) y, (float) z, (float) r2a);
+      qa[slot] = make_float4(d.x, d.y, d.z, r2);
       const float4 *src = a.site + 3 * (size_t) jc;
       cp_async16(&q0[slot], src);
-      cp_async16(&q1[slot], src + 1);
-      cp_async16(&q2[slot], src + 2);
+      if (UNI) {
+        cp_async8(&q1[slot], src + 1);  // the H z offsets; the charges are the arguments'
+      } else {
+        cp_async16(&q1[slot], src + 1);
+        cp_async16(&q2[slot], src + 2);
+      }
     }
     cp_async_commit();
     // entries of earlier batches are evaluated one batch after their copies
@@ -732,6 +787,8 @@ __device__ __forceinline__ int water_row(const WaterArgs &a, int p, int lane, fl
     if (lane < qn)
       compute((head + lane) & kMask);
   if (make && lane == 0) {
+    // the anchors at this prune (FP64: the list check measures moves from them)
+    const double4 ai = a.anchor[p];
     a.pcount[p] = pn;
     a.plast[3 * p] = ai.x;
     a.plast[3 * p + 1] = ai.y;
@@ -785,7 +842,7 @@ __device__ __forceinline__ void water_row_store_shfl(const WaterArgs &a, int si0
 // registers, 5: 96); mmnb_autotune picks per handle
 // VIR: also the part of dU/ds (box scaling) the site forces do not carry, the
 // anchor force scalar times R^2 per group pair (mmnb_virial)
-template <int MINB, bool VIR>
+template <int MINB, bool VIR, bool UNI>
 __global__ void __launch_bounds__(kWaterWarps * 32, MINB * kMxWarps / kWaterWarps) k_pair_water(WaterArgs a)
 {
   // per warp: ring of anchor displacement (xyz, r^2) and the partner's three
@@ -801,7 +858,7 @@ __global__ void __launch_bounds__(kWaterWarps * 32, MINB * kMxWarps / kWaterWarp
 #pragma unroll
     for (int c = 0; c < kCols; c++)
       fx[c] = 0;
-    const int si0 = water_row<VIR>(a, p, lane, ring[w][0], ring[w][1], ring[w][2], ring[w][3], fx);
+    const int si0 = water_row<VIR, UNI>(a, p, lane, ring[w][0], ring[w][1], ring[w][2], ring[w][3], fx);
     water_row_store_shfl<VIR>(a, si0, lane, fx, te, tl, tv);
   }
   if (a.pnbr && a.flags[kFlagPruneFull] && blockIdx.x == 0 && threadIdx.x == 0)
@@ -852,14 +909,35 @@ cudaError_t launch_rspace_water(mmnb_handle *h)
   a.plast = h->d_plast;
   a.flags = h->d_flags;
   a.rp2 = (h->rc + h->prune_margin) * (h->rc + h->prune_margin);
+  a.anc32 = h->mx.anc32;
+  a.ncell = h->cg.n;
+  a.nhalf = h->cg.n / 2;
+  for (int d = 0; d < 3; d++) {
+    a.edge[d] = (float) h->cg.lc[d];
+    a.Lf[d] = (float) h->box.L[d];
+    a.halfL[d] = (float) (0.5 * h->box.L[d]);
+  }
+  a.rhi2f = (float) a.rhi2;
+  a.rp2f = (float) a.rp2;
+  a.uqO = h->uni_qO;
+  a.uqH = h->uni_qH;
+  a.usig = h->uni_sig;
+  a.useps = h->uni_seps;
   h->launches += 1;
   const int blocks = div_up(h->ngroup, kWaterWarps);
-  if (h->want_virial)
-    k_pair_water<4, true><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
+  const bool uni = h->water_uni;
+  if (h->want_virial && uni)
+    k_pair_water<4, true, true><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
+  else if (h->want_virial)
+    k_pair_water<4, true, false><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
+  else if (h->tune.water_minb == 5 && uni)
+    k_pair_water<5, false, true><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
   else if (h->tune.water_minb == 5)
-    k_pair_water<5, false><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
+    k_pair_water<5, false, false><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
+  else if (uni)
+    k_pair_water<4, false, true><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
   else
-    k_pair_water<4, false><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
+    k_pair_water<4, false, false><<<blocks, kWaterWarps * 32, 0, h->stream>>>(a);
   return cudaGetLastError();
 }
 
@@ -874,7 +952,8 @@ __global__ void k_prep_mixed(const double *__restrict__ r, const double *__restr
                              const int *__restrict__ sorted, const int *__restrict__ group, int ngroup, int G,
                              int water, float4 *__restrict__ site, float4 *__restrict__ par,
                              double4 *__restrict__ anchor, unsigned long long *__restrict__ wsum,
-                             int *__restrict__ flags)
+                             int *__restrict__ flags, float4 *__restrict__ anc32, Box box, int ncell,
+                             double3 edge)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < 2)
@@ -895,6 +974,22 @@ __global__ void k_prep_mixed(const double *__restrict__ r, const double *__restr
       !isfinite(r[3 * (a0 + k)] + r[3 * (a0 + k) + 1] + r[3 * (a0 + k) + 2]))
     flags[kFlagError] = MMNB_ERR_DEVICE;
   if (water) {
+    if (k == 0) {
+      // the anchor wrapped into the box, its list cell (edge as the kernel
+      // holds it, in FP32) and its offset from that cell's corner
+      const double av[3] = {ax, ay, az}, ev[3] = {edge.x, edge.y, edge.z};
+      float o[3];
+      int code = 0;
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const double wv = av[d] - box.L[d] * floor(av[d] * box.invL[d]);
+        int c = (int) floor(wv / ev[d]);
+        c = min(max(c, 0), ncell - 1);
+        o[d] = (float) (wv - c * ev[d]);
+        code |= c << (10 * d);
+      }
+      anc32[p] = make_float4(o[0], o[1], o[2], __int_as_float(code));
+    }
     // G == 3: slot k of group p from the two H sites (a0 + 1, a0 + 2) and O
     const int h1 = a0 + 1, h2 = a0 + 2;
     float4 v;
@@ -923,9 +1018,11 @@ cudaError_t launch_prep_mixed(mmnb_handle *h, const double *d_r)
 {
   const int n = h->ngroup * h->G;
   const int water = h->water && !h->want_fields && h->cfg.include_rspace;
+  const double3 edge = make_double3((float) h->cg.lc[0], (float) h->cg.lc[1], (float) h->cg.lc[2]);
   k_prep_mixed<<<div_up(n, 256), 256, 0, h->stream>>>(d_r, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_mask,
                                                       h->d_sorted, h->d_group, h->ngroup, h->G, water, h->mx.site,
-                                                      h->mx.par, h->mx.anchor, h->d_wsum, h->d_flags);
+                                                      h->mx.par, h->mx.anchor, h->d_wsum, h->d_flags, h->mx.anc32,
+                                                      h->box, h->cg.n, edge);
   h->launches += 1;
   return cudaGetLastError();
 }
