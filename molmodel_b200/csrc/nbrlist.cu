@@ -106,7 +106,9 @@ __global__ void __launch_bounds__(kCheckThreads) k_list_check(const double *__re
     const double dx = __dsub_rn(x, last[3 * g]);
     const double dy = __dsub_rn(y, last[3 * g + 1]);
     const double dz = __dsub_rn(z, last[3 * g + 2]);
-    const double d = __dsqrt_rn(exact_sq3(dx, dy, dz));
+    // squared moves: the square root (monotonic, correctly rounded) is
+    // taken of the two largest only, in the last block
+    const double d = exact_sq3(dx, dy, dz);
     if (d > a) {
       b = a;
       a = d;
@@ -116,7 +118,7 @@ __global__ void __launch_bounds__(kCheckThreads) k_list_check(const double *__re
     if (prune > 0) {
       const int p = rank[g];
       const double ex = x - plast[3 * p], ey = y - plast[3 * p + 1], ez = z - plast[3 * p + 2];
-      const double e = sqrt(ex * ex + ey * ey + ez * ez);
+      const double e = ex * ex + ey * ey + ez * ez;
       if (e > pa) {
         pb = pa;
         pa = e;
@@ -147,6 +149,10 @@ __global__ void __launch_bounds__(kCheckThreads) k_list_check(const double *__re
   }
   block_top2(a, b, sa, sb);
   block_top2(pa, pb, sa, sb);
+  a = __dsqrt_rn(a);
+  b = __dsqrt_rn(b);
+  pa = sqrt(pa);
+  pb = sqrt(pb);
   __shared__ int rebuild_s;
   if (threadIdx.x == 0) {
     const int count = flags[4];

@@ -953,7 +953,7 @@ __global__ void k_prep_mixed(const double *__restrict__ r, const double *__restr
                              int water, float4 *__restrict__ site, float4 *__restrict__ par,
                              double4 *__restrict__ anchor, unsigned long long *__restrict__ wsum,
                              int *__restrict__ flags, float4 *__restrict__ anc32, Box box, int ncell,
-                             double3 edge)
+                             double3 edge, double3 inv_edge)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < 2)
@@ -977,13 +977,15 @@ __global__ void k_prep_mixed(const double *__restrict__ r, const double *__restr
     if (k == 0) {
       // the anchor wrapped into the box, its list cell (edge as the kernel
       // holds it, in FP32) and its offset from that cell's corner
-      const double av[3] = {ax, ay, az}, ev[3] = {edge.x, edge.y, edge.z};
+      // (any cell near the anchor serves: the offset is taken from the cell
+      // chosen, so the cell index needs no exact division)
+      const double av[3] = {ax, ay, az}, ev[3] = {edge.x, edge.y, edge.z}, iv[3] = {inv_edge.x, inv_edge.y, inv_edge.z};
       float o[3];
       int code = 0;
 #pragma unroll
       for (int d = 0; d < 3; d++) {
         const double wv = av[d] - box.L[d] * floor(av[d] * box.invL[d]);
-        int c = (int) floor(wv / ev[d]);
+        int c = (int) floor(wv * iv[d]);
         c = min(max(c, 0), ncell - 1);
         o[d] = (float) (wv - c * ev[d]);
         code |= c << (10 * d);
@@ -1019,10 +1021,11 @@ cudaError_t launch_prep_mixed(mmnb_handle *h, const double *d_r)
   const int n = h->ngroup * h->G;
   const int water = h->water && !h->want_fields && h->cfg.include_rspace;
   const double3 edge = make_double3((float) h->cg.lc[0], (float) h->cg.lc[1], (float) h->cg.lc[2]);
+  const double3 inv_edge = make_double3(1.0 / edge.x, 1.0 / edge.y, 1.0 / edge.z);
   k_prep_mixed<<<div_up(n, 256), 256, 0, h->stream>>>(d_r, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_mask,
                                                       h->d_sorted, h->d_group, h->ngroup, h->G, water, h->mx.site,
                                                       h->mx.par, h->mx.anchor, h->d_wsum, h->d_flags, h->mx.anc32,
-                                                      h->box, h->cg.n, edge);
+                                                      h->box, h->cg.n, edge, inv_edge);
   h->launches += 1;
   return cudaGetLastError();
 }
