@@ -135,6 +135,7 @@ struct mmnb_handle {
   // 512 x 4: the cubics of -eta d/d(eta) of the table (mmnb_virial)
   double *d_cheb_d = nullptr;
   int water64_grid = 0;              // persistent blocks of that kernel (0: not sized yet)
+  int water64_warps = 0;             // warps per block of that kernel
   size_t water64_smem = 0;
 
   // neighbour list

@@ -23,7 +23,7 @@
 //     absolute at those distances), and below its lower end (r^2 < 4) erfc and
 //     exp are evaluated directly, as in the reference.
 //
-// Layout: a persistent grid, one block of kW64Warps warps per SM slot; each
+// Layout: a persistent grid, one block of up to kW64Warps warps per SM slot; each
 // warp takes the next row group from a counter and walks its list 32 entries
 // at a time (anchor test per lane, ballot compaction into a 128-slot ring of
 // anchor displacements, cp.async of the partner's 96-byte record into the same
@@ -40,8 +40,11 @@ namespace mmnb {
 #ifndef MMNB_W64_BLOCKS
 #define MMNB_W64_BLOCKS 1
 #endif
+// warps per block the kernel is compiled for (its register budget: 12 warps
+// of 384 threads leave 170 registers a thread); a launch may use fewer when
+// the rings and the table do not fit in shared memory
 #ifndef MMNB_W64_WARPS
-#define MMNB_W64_WARPS 8
+#define MMNB_W64_WARPS 12
 #endif
 constexpr int kW64Warps = MMNB_W64_WARPS;
 // a batch of 32 is queued before the oldest 32 are evaluated, so the ring
@@ -130,7 +133,7 @@ __global__ void __launch_bounds__(kW64Warps * 32, MMNB_W64_BLOCKS) k_pair_water6
   extern __shared__ __align__(16) unsigned char smem[];
   // per warp: ring of (anchor displacement, r^2) and the partner's record
   double4 *ring = reinterpret_cast<double4 *>(smem);  // [warps][4][kW64Ring]
-  double2 *tc01 = reinterpret_cast<double2 *>(smem + sizeof(double4) * 4 * kW64Ring * kW64Warps);
+  double2 *tc01 = reinterpret_cast<double2 *>(smem + sizeof(double4) * 4 * kW64Ring * (blockDim.x >> 5));
   const double2 *tc23 = tc01 + a.nseg;
   for (int i = threadIdx.x; i < 2 * a.nseg; i += blockDim.x)
     tc01[i] = a.table[i];
@@ -323,9 +326,9 @@ __global__ void k_sort_water64(const double *__restrict__ r, const double *__res
   rec[3 * (size_t) p + 2] = make_double4(q[a0 + 2], sig[a0], sqrt(eps[a0]), 0.0);
 }
 
-static size_t water64_smem(const mmnb_handle *h)
+static size_t water64_smem(const mmnb_handle *h, int warps)
 {
-  return sizeof(double4) * 4 * kW64Ring * kW64Warps + sizeof(double2) * 2 * (size_t) h->cheb_w_nseg;
+  return sizeof(double4) * 4 * kW64Ring * warps + sizeof(double2) * 2 * (size_t) h->cheb_w_nseg;
 }
 
 cudaError_t launch_sort_water64(mmnb_handle *h, const double *d_r)
@@ -339,26 +342,35 @@ cudaError_t launch_sort_water64(mmnb_handle *h, const double *d_r)
 
 cudaError_t launch_rspace_water64(mmnb_handle *h)
 {
-  const size_t smem = water64_smem(h);
   if (h->water64_grid == 0) {
     cudaError_t e;
+    int optin = 0, nsm = 0;
+    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->dev)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->dev)) != cudaSuccess)
+      return e;
+    // as many warps as the rings and this box's table leave room for (the
+    // table grows with rc: 12 warps below ~22 KB of table, fewer above)
+    int warps = kW64Warps;
+    while (warps > 4 && water64_smem(h, warps) > (size_t) optin)
+      warps -= 2;
+    const size_t smem = water64_smem(h, warps);
     if ((e = cudaFuncSetAttribute(k_pair_water64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)) !=
             cudaSuccess ||
         (e = cudaFuncSetAttribute(k_pair_water64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)) !=
             cudaSuccess)
       return e;
-    int per_sm = 0, per_sm_v = 0, nsm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_water64<false>, kW64Warps * 32, smem)) !=
+    int per_sm = 0, per_sm_v = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_water64<false>, warps * 32, smem)) !=
             cudaSuccess ||
-        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_v, k_pair_water64<true>, kW64Warps * 32, smem)) !=
-            cudaSuccess ||
-        (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->dev)) != cudaSuccess)
+        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_v, k_pair_water64<true>, warps * 32, smem)) !=
+            cudaSuccess)
       return e;
     per_sm = std::min(per_sm, per_sm_v);
     if (per_sm < 1)
       return cudaErrorLaunchOutOfResources;
-    h->water64_grid = std::min(per_sm * nsm, div_up(h->ngroup, kW64Warps));
+    h->water64_grid = std::min(per_sm * nsm, div_up(h->ngroup, warps));
     h->water64_smem = smem;
+    h->water64_warps = warps;
   }
   Water64Args a;
   a.ngroup = h->ngroup;
@@ -389,9 +401,9 @@ cudaError_t launch_rspace_water64(mmnb_handle *h)
   a.vir_row = h->want_virial ? h->d_vir_row : nullptr;
   a.cheb_d = h->d_cheb_d;
   if (h->want_virial)
-    k_pair_water64<true><<<h->water64_grid, kW64Warps * 32, h->water64_smem, h->stream>>>(a);
+    k_pair_water64<true><<<h->water64_grid, h->water64_warps * 32, h->water64_smem, h->stream>>>(a);
   else
-    k_pair_water64<false><<<h->water64_grid, kW64Warps * 32, h->water64_smem, h->stream>>>(a);
+    k_pair_water64<false><<<h->water64_grid, h->water64_warps * 32, h->water64_smem, h->stream>>>(a);
   h->launches += 1;
   return cudaGetLastError();
 }
