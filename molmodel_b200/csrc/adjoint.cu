@@ -366,14 +366,12 @@ static int grad_p3m_scratch(mmnb_handle *h, P3mScratch &s)
     }
     return MMNB_OK;
   }
-  if (h->cfg.p3m_ik_differentiate) {
-    h->err = "ik differentiation in the mixed form";
-    return MMNB_ERR_UNSUPPORTED;
-  }
+  // ik: three spread meshes and the summed spectrum's mesh
+  const int nm = h->cfg.p3m_ik_differentiate ? 4 : 1;
   if (!h->gplan_r2c) {
-    cudaError_t e = cudaMalloc(&h->d_gmesh, sizeof(double) * nr);
+    cudaError_t e = cudaMalloc(&h->d_gmesh, sizeof(double) * nr * nm);
     if (e == cudaSuccess)
-      e = cudaMalloc(&h->d_gmeshk, sizeof(cufftDoubleComplex) * nk);
+      e = cudaMalloc(&h->d_gmeshk, sizeof(cufftDoubleComplex) * nk * nm);
     if (e != cudaSuccess) {
       h->err = std::string("gradient mesh: ") + cudaGetErrorString(e);
       return MMNB_ERR_CUDA;
@@ -386,8 +384,14 @@ static int grad_p3m_scratch(mmnb_handle *h, P3mScratch &s)
   }
   s.r2c = h->gplan_r2c;
   s.c2r = h->gplan_c2r;
-  s.spread = s.solve = h->d_gmesh;
+  s.spread = h->d_gmesh;
   s.spreadk = h->d_gmeshk;
+  if (nm == 4) {
+    s.solve = h->d_gmesh + 3 * nr;
+    s.solvek = h->d_gmeshk + 3 * nk;
+  } else {
+    s.solve = h->d_gmesh;
+  }
   return MMNB_OK;
 }
 

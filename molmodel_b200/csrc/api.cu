@@ -390,6 +390,9 @@ int setup_p3m(mmnb_handle *h)
         (s = dalloc(h, &h->d_meshk32, nk)) || (s = dalloc(h, &h->d_green32, nk)))
       return s;
     CK(cudaMemset(h->d_mesh_fx, 0, sizeof(unsigned long long) * nr));
+    if (c.p3m_ik_differentiate)
+      if ((s = dalloc(h, &h->d_egrid32, 3 * nr)) || (s = dalloc(h, &h->d_egridk32, 3 * nk)))
+        return s;
     CKFFT(cufftPlan3d(&h->plan_r2c32, h->mesh[0], h->mesh[1], h->mesh[2], CUFFT_R2C));
     CKFFT(cufftPlan3d(&h->plan_c2r32, h->mesh[0], h->mesh[1], h->mesh[2], CUFFT_C2R));
     CKFFT(cufftSetStream(h->plan_r2c32, h->stream));
@@ -437,7 +440,7 @@ void free_all(mmnb_handle *h)
                   h->d_sp, h->d_site_of_slot,
                   h->d_phi, h->d_evec, h->d_ljf, h->d_lj_part, h->d_elec_part, h->d_energy, h->d_r, h->d_f,
                   h->d_mesh, h->d_meshk, h->d_green, h->d_kvec, h->d_egrid, h->d_egridk, h->d_mesh32,
-                  h->d_meshk32, h->d_green32, h->d_mesh_fx, h->d_kint, h->d_kvecs, h->d_ak, h->d_skc,
+                  h->d_meshk32, h->d_green32, h->d_egrid32, h->d_egridk32, h->d_mesh_fx, h->d_kint, h->d_kvecs, h->d_ak, h->d_skc,
                   h->mx.site, h->mx.par, h->mx.anchor, h->mx.anc32, h->mx.acc, h->mx.acck, h->d_wsum,
                   h->d_bwd, h->d_gmesh, h->d_gmeshk};
   for (void *p : ptrs)
@@ -628,8 +631,6 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
   h->rhi2 = sq(h->rc);
   h->rlo2 = sq(h->rc - c->smoothing_width);
   h->inv_sw = h->rhi2 > h->rlo2 ? 1.0 / (h->rhi2 - h->rlo2) : 0.0;
-  if (c->precision == MMNB_MIXED && c->use_p3m && c->p3m_ik_differentiate)
-    return fail(h, MMNB_ERR_UNSUPPORTED, "the mixed form differentiates P3M in real space only");
   // Ewald parameter (src/eleclj.cpp:189-239)
   h->eta = c->ewald_screening;
   if (c->include_kspace && c->use_p3m) {

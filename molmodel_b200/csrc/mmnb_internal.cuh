@@ -242,6 +242,8 @@ struct mmnb_handle {
   float *d_mesh32 = nullptr;
   cufftComplex *d_meshk32 = nullptr;
   float *d_green32 = nullptr;
+  float *d_egrid32 = nullptr;        // ik differentiation: three FP32 field meshes
+  cufftComplex *d_egridk32 = nullptr;
   unsigned long long *d_mesh_fx = nullptr;
 
   // ordinary Ewald

@@ -705,6 +705,25 @@ __global__ void k_green_mul32(long nk, const float *__restrict__ green, cufftCom
   meshk[g] = v;
 }
 
+// ik differentiation: the potential spectrum G rho^ in place and the three
+// field spectra -i k_d G rho^ (the FP64 form's k_green_mul, in FP32)
+__global__ void k_green_mul32_ik(long nk, const float *__restrict__ green, const double *__restrict__ kvec,
+                                 cufftComplex *__restrict__ meshk, cufftComplex *__restrict__ egk)
+{
+  const long g = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nk)
+    return;
+  const float a = green[g];
+  cufftComplex v = meshk[g];
+  v.x *= a;
+  v.y *= a;
+  meshk[g] = v;
+  for (int d = 0; d < 3; d++) {
+    const float k = (float) kvec[3 * g + d];
+    egk[d * nk + g] = make_cuComplex(k * v.y, -k * v.x);
+  }
+}
+
 __global__ void k_green_to_f32(long nk, const double *__restrict__ green, float *__restrict__ out)
 {
   const long g = (long) blockIdx.x * blockDim.x + threadIdx.x;
@@ -768,6 +787,57 @@ __global__ void k_gather_mixed(MeshArgs m, const double *__restrict__ r, int nsi
   reinterpret_cast<longlong4 *>(acck)[i] = o;
 }
 
+// ik differentiation: the potential and the three field components
+// interpolated with the assignment weights (the field meshes are already the
+// Cartesian field), into the same fixed-point words as k_gather_mixed
+template <int P>
+__global__ void k_gather_mixed_ik(MeshArgs m, const double *__restrict__ r, int nsite, const float *__restrict__ mesh,
+                                  const float *__restrict__ egrid, size_t nr, long long *__restrict__ acck)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nsite)
+    return;
+  const double x = r[3 * i], y = r[3 * i + 1], z = r[3 * i + 2];
+  float W[3][P], ND[3][P];
+  int base[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    double w;
+    base[d] = bspline_base<P>(m.A[d] * x + m.A[3 + d] * y + m.A[6 + d] * z, w);
+    bspline_eval<P, float>((float) w, W[d], ND[d]);
+  }
+  int iy_[P], iz_[P];
+#pragma unroll
+  for (int p = 0; p < P; p++) {
+    iy_[p] = wrap_idx(base[1] + p, m.n[1]);
+    iz_[p] = wrap_idx(base[2] + p, m.n[2]);
+  }
+  float ph = 0.f, ex = 0.f, ey = 0.f, ez = 0.f;
+  for (int a = 0; a < P; a++) {
+    const int ix = wrap_idx(base[0] + a, m.n[0]);
+#pragma unroll
+    for (int b = 0; b < P; b++) {
+      const size_t rowoff = ((size_t) ix * m.n[1] + iy_[b]) * m.n[2];
+      const float wxy = W[0][a] * W[1][b];
+#pragma unroll
+      for (int c = 0; c < P; c++) {
+        const size_t k = rowoff + iz_[c];
+        const float ww = wxy * W[2][c];
+        ph = fmaf(ww, __ldg(mesh + k), ph);
+        ex = fmaf(ww, __ldg(egrid + k), ex);
+        ey = fmaf(ww, __ldg(egrid + nr + k), ey);
+        ez = fmaf(ww, __ldg(egrid + 2 * nr + k), ez);
+      }
+    }
+  }
+  longlong4 o;
+  o.x = __float2ll_rn(ph * 4294967296.0f);
+  o.y = __float2ll_rn(ex * 4294967296.0f);
+  o.z = __float2ll_rn(ey * 4294967296.0f);
+  o.w = __float2ll_rn(ez * 4294967296.0f);
+  reinterpret_cast<longlong4 *>(acck)[i] = o;
+}
+
 cudaError_t launch_green32(mmnb_handle *h)
 {
   const long nk = (long) h->mesh[0] * h->mesh[1] * (h->mesh[2] / 2 + 1);
@@ -797,14 +867,26 @@ static cudaError_t p3m_mixed_p(mmnb_handle *h, const double *d_r, int stage)
         cufftSetStream(h->plan_c2r32, h->stream) != CUFFT_SUCCESS ||
         cufftExecR2C(h->plan_r2c32, h->d_mesh32, h->d_meshk32) != CUFFT_SUCCESS)
       return cudaErrorUnknown;
-    k_green_mul32<<<div_up(nk, 256), 256, 0, h->stream>>>(nk, h->d_green32, h->d_meshk32);
+    if (h->d_egrid32) {
+      k_green_mul32_ik<<<div_up(nk, 256), 256, 0, h->stream>>>(nk, h->d_green32, h->d_kvec, h->d_meshk32,
+                                                               h->d_egridk32);
+      for (int d = 0; d < 3; d++)
+        if (cufftExecC2R(h->plan_c2r32, h->d_egridk32 + d * nk, h->d_egrid32 + d * nr) != CUFFT_SUCCESS)
+          return cudaErrorUnknown;
+    } else {
+      k_green_mul32<<<div_up(nk, 256), 256, 0, h->stream>>>(nk, h->d_green32, h->d_meshk32);
+    }
     if (cufftExecC2R(h->plan_c2r32, h->d_meshk32, h->d_mesh32) != CUFFT_SUCCESS)
       return cudaErrorUnknown;
     timing_mark(h, "p3m_fft");
     h->launches += 3;
   }
   if (stage & 2) {
-    k_gather_mixed<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->nsite, h->d_mesh32, h->mx.acck);
+    if (h->d_egrid32)
+      k_gather_mixed_ik<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->nsite, h->d_mesh32,
+                                                                          h->d_egrid32, nr, h->mx.acck);
+    else
+      k_gather_mixed<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->nsite, h->d_mesh32, h->mx.acck);
     timing_mark(h, "p3m_gather");
     h->launches += 1;
   }

@@ -157,8 +157,6 @@ def test_mixed_site_gradients_match_fp64_for_the_same_loss_gradient(case):
     one only through the forward's site potentials and fields (FP32 pair
     arithmetic): 2e-5 of the largest term."""
     name, s, cfg, targets, checks = case
-    if cfg.get("p3m_ik_differentiate"):
-        pytest.skip("ik differentiation is FP64 only")
     out64, g64 = site_grads(s, cfg, "fp64", targets)
     dl_df = 2 * (out64["f"] - targets)
     _, gm = site_grads(s, cfg, "mixed", targets, dl_df=dl_df)

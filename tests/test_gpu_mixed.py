@@ -48,6 +48,22 @@ def test_mixed_error_vs_fp64_oracle(n, mesh, seed, fields):
     assert abs(g["elec"] - o["elec"]) < ENERGY_TOL * abs(o["elec"])
 
 
+@pytest.mark.parametrize("fields", [False, True], ids=["water-kernel", "general-kernel"])
+@pytest.mark.parametrize("order", [3, 5, 7])
+def test_mixed_p3m_ik_differentiation(order, fields):
+    """P3M with ik differentiation (src/pppm.c:567-601): the three field
+    meshes -ik G rho^ in FP32, interpolated with the assignment weights."""
+    wb = water_box(8, seed=4)
+    cfg = p3m(wb.box, 24, p3m_assignment_order=order, p3m_ik_differentiate=True, neighbor_list_width=1.5)
+    g = ElecLJ(precision="mixed", **cfg).init(wb).compute(wb.positions, want_fields=fields)
+    o = oracle_eval(wb, cfg)
+    assert rel_rms(g["f"], o["f"]) < RMS_TOL
+    assert rel_max(g["f"], o["f"]) < MAX_TOL
+    assert abs(g["total"] - o["total"]) < ENERGY_TOL * abs(o["total"])
+    if fields:
+        assert rel_rms(g["evec"], o["evec"]) < RMS_TOL
+
+
 @pytest.mark.parametrize("order", [2, 3, 4, 5, 6, 7])
 @pytest.mark.parametrize("mesh", [18, 20])
 def test_mixed_p3m_orders(mesh, order):
