@@ -285,7 +285,8 @@ def run_ours(args):
                       "launch": "CUDA graph of one evaluation, replayed per step",
                       "tuning": {"water_kernel_registers": 128 if tuning[0] == 4 else 96, "spread_layout":
                                  ("thread per site", "thread per site and x-plane",
-                                  "lane per site and z-offset")[tuning[1]], "p3m_side_stream": bool(tuning[2])}},
+                                  "lane per site and z-offset")[tuning[1]], "p3m_side_stream": bool(tuning[2]),
+                                 "fp64_water_warps_per_block": tuning[3]}},
            "ms_per_step_without_graph": nograph_ms / args.steps,
            "pair_evals_per_s": work["coulomb_site_pairs"] * steps_per_s,
            "ns_per_day": steps_per_s / world * DT_FS * 86400 / 1e6,

@@ -265,13 +265,15 @@ int mmnb_measure_fp32_peak(int device, double *tflops);
    site and mesh x-plane, 2 (default): a lane per site and mesh z-offset, so
    the lanes of a site reduce into consecutive mesh words),
    tuning[2] = P3M mesh work on a second stream beside the pair kernels (1) or
-   in line (0).  mmnb_autotune times each choice over `iters` graph replays of
+   in line (0), tuning[3] = warps per block of the FP64 rigid-water kernel
+   (12, 10 or 8; fewer are launched when its rings and the box's erfc table do
+   not fit in shared memory).  mmnb_autotune times each choice over `iters` graph replays of
    an evaluation at r (host array) and keeps the fastest; small systems gain
    most.  It evaluates at r (advancing the rebuild counters); a graph captured
    with mmnb_graph_capture before tuning keeps the old choices. */
 int mmnb_autotune(mmnb_handle *h, const double *r, int iters);
-int mmnb_get_tuning(mmnb_handle *h, int tuning[3]);
-int mmnb_set_tuning(mmnb_handle *h, const int tuning[3]);
+int mmnb_get_tuning(mmnb_handle *h, int tuning[4]);
+int mmnb_set_tuning(mmnb_handle *h, const int tuning[4]);
 
 /* ---- adjoint --------------------------------------------------------------
    Per-site parameter gradients, for the force-field fits the reference runs

@@ -1571,9 +1571,10 @@ int mmnb_autotune(mmnb_handle *h, const double *r, int iters)
     int nval;
     int vals[3];
     bool on;
-  } knobs[] = {{&h->tune.water_minb, 2, {4, 5}, mixed && h->water},
+  } knobs[] = {{&h->tune.water_minb, 2, {5, 4}, mixed && h->water},
                {&h->tune.spread_planes, 3, {2, 0, 1}, mixed && p3m},
-               {&h->tune.p3m_side, 2, {1, 0}, p3m}};
+               {&h->tune.p3m_side, 2, {1, 0}, p3m},
+               {&h->tune.water64_warps, 3, {12, 10, 8}, !mixed && h->water && h->cfg.include_rspace}};
   for (Knob &k : knobs) {
     if (!k.on)
       continue;
@@ -1596,24 +1597,28 @@ int mmnb_autotune(mmnb_handle *h, const double *r, int iters)
   return MMNB_OK;
 }
 
-int mmnb_get_tuning(mmnb_handle *h, int tuning[3])
+int mmnb_get_tuning(mmnb_handle *h, int tuning[4])
 {
   if (!h || !tuning)
     return MMNB_ERR_ARG;
   tuning[0] = h->tune.water_minb;
   tuning[1] = h->tune.spread_planes;
   tuning[2] = h->tune.p3m_side;
+  tuning[3] = h->tune.water64_warps;
   return MMNB_OK;
 }
 
-int mmnb_set_tuning(mmnb_handle *h, const int tuning[3])
+int mmnb_set_tuning(mmnb_handle *h, const int tuning[4])
 {
   if (!h || !tuning || (tuning[0] != 4 && tuning[0] != 5) || tuning[1] < 0 || tuning[1] > 2 ||
-      (tuning[2] != 0 && tuning[2] != 1))
-    return fail(h, MMNB_ERR_ARG, "tuning values: water blocks 4 or 5, spread layout 0, 1 or 2, P3M side 0 or 1");
+      (tuning[2] != 0 && tuning[2] != 1) || (tuning[3] != 8 && tuning[3] != 10 && tuning[3] != 12))
+    return fail(h, MMNB_ERR_ARG,
+                "tuning values: water blocks 4 or 5, spread layout 0, 1 or 2, P3M side 0 or 1, FP64 water warps "
+                "8, 10 or 12");
   h->tune.water_minb = tuning[0];
   h->tune.spread_planes = tuning[1];
   h->tune.p3m_side = tuning[2];
+  h->tune.water64_warps = tuning[3];
   drop_host_graph(h);
   return MMNB_OK;
 }

@@ -53,10 +53,12 @@ constexpr int kAccStride = 8;  // phi, Ex, Ey, Ez, Lx, Ly, Lz, (pad) per site
 
 // Launch choices that do not change any result (mmnb_autotune times them).
 struct Tuning {
-  int water_minb = 4;      // rigid-water pair kernel: 4 or 5 resident blocks per SM
+  int water_minb = 5;      // rigid-water pair kernel: 4 or 5 resident warps per SM / 4 (128 or 96 registers)
   int spread_planes = 2;   // mixed P3M spread: 0 one thread per site, 1 P threads per site (x planes),
                            // 2 P lanes per site along z (coalesced reductions)
   int p3m_side = 1;        // P3M mesh work on the side stream (1) or in line (0)
+  int water64_warps = 12;  // FP64 rigid-water kernel: warps per block (12, 10 or 8; fewer when the
+                           // rings and the table do not fit in shared memory)
 };
 
 // Device buffers of the mixed-precision form.

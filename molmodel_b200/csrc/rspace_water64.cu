@@ -342,17 +342,19 @@ cudaError_t launch_sort_water64(mmnb_handle *h, const double *d_r)
 
 cudaError_t launch_rspace_water64(mmnb_handle *h)
 {
-  if (h->water64_grid == 0) {
-    cudaError_t e;
-    int optin = 0, nsm = 0;
-    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->dev)) != cudaSuccess ||
-        (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->dev)) != cudaSuccess)
+  cudaError_t e;
+  int optin = 0;
+  if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->dev)) != cudaSuccess)
+    return e;
+  // the tuned warps per block, fewer if the rings and this box's table do not
+  // fit (the table grows with rc: 12 warps below ~22 KB of table)
+  int warps = std::min(h->tune.water64_warps, kW64Warps);
+  while (warps > 4 && water64_smem(h, warps) > (size_t) optin)
+    warps -= 2;
+  if (h->water64_grid == 0 || warps != h->water64_warps) {
+    int nsm = 0;
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->dev)) != cudaSuccess)
       return e;
-    // as many warps as the rings and this box's table leave room for (the
-    // table grows with rc: 12 warps below ~22 KB of table, fewer above)
-    int warps = kW64Warps;
-    while (warps > 4 && water64_smem(h, warps) > (size_t) optin)
-      warps -= 2;
     const size_t smem = water64_smem(h, warps);
     if ((e = cudaFuncSetAttribute(k_pair_water64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)) !=
             cudaSuccess ||

@@ -213,20 +213,27 @@ class ElecLJ:
 
     def autotune(self, r, iters=10):
         """Time the launch choices at positions r and keep the fastest;
-        returns them (water-kernel register budget code, spread layout, P3M stream)."""
+        returns them (see tuning)."""
         r = np.ascontiguousarray(r, dtype=np.float64)
         check(load().mmnb_autotune(self._h, _d(r), int(iters)), self._h)
         return self.tuning
 
     @property
     def tuning(self):
-        t = np.zeros(3, dtype=np.int32)
+        """(water kernel register budget code, spread layout, P3M side stream,
+        FP64 water kernel warps per block), see mmnb_get_tuning."""
+        t = np.zeros(4, dtype=np.int32)
         check(load().mmnb_get_tuning(self._h, _i(t)), self._h)
         return tuple(int(x) for x in t)
 
     @tuning.setter
     def tuning(self, values):
+        values = list(values)
+        if len(values) == 3:  # the FP64 choice kept
+            values.append(self.tuning[3])
         t = np.ascontiguousarray(values, dtype=np.int32)
+        if t.shape != (4,):
+            raise ValueError("tuning takes 3 or 4 values")
         check(load().mmnb_set_tuning(self._h, _i(t)), self._h)
 
     def compute_device(self, d_r, d_f, d_energy):

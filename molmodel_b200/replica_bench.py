@@ -13,7 +13,7 @@ reproducible.  Under torchrun (one process per GPU, NCCL) the replicas are
 spread over the ranks by longest processing time on their site counts and the
 ranks meet once per exchange (molmodel_b200.remd.ReplicaExchange).
 
-  python -m molmodel_b200.replica_bench [--replicas 64] [--steps 1000] [--interval 500]
+  python -m molmodel_b200.replica_bench [--replicas 64] [--steps 1000] [--interval 500] [--merged]
   torchrun --nproc-per-node N -m molmodel_b200.replica_bench ...
 """
 import argparse
@@ -56,6 +56,9 @@ def main():
     ap.add_argument("--precision", default="mixed")
     ap.add_argument("--no-sequential", action="store_true")
     ap.add_argument("--autotune", action="store_true", help="tune each replica's launch choices first")
+    ap.add_argument("--merged", action="store_true",
+                    help="also time one box holding all the replicas' waters (the bound a single fused launch "
+                         "over the replicas could approach)")
     args = ap.parse_args()
     import torch
     rank, world = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
@@ -115,6 +118,29 @@ def main():
         out.update(sequential_s_estimate=t_seq, batching_speedup=t_seq / t_batch)
     batch.close()
     for _, pot, md in reps.values():
+        md.close()
+        pot.close()
+    if args.merged and world == 1:
+        # one box with the same total number of waters and the same settings:
+        # every kernel of a step is one launch over all of them, so its
+        # water-steps per second bound what fusing the replicas' launches
+        # into persistent kernels could reach
+        total = sum(sizes)
+        wb = water_box_n(total, seed=77)
+        pot = ElecLJ(precision=args.precision, rspace_cutoff=9.0, ewald_screening=0.35, neighbor_list_width=1.5,
+                     use_p3m=True, p3m_grid_spacing=1.04, p3m_assignment_order=5).init(wb)
+        md = MDyn(pot, wb.masses, timestep=0.002)
+        md.set_state(wb.positions, maxwell_boltzmann(wb, 300.0, seed=78))
+        md.run(20)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        md.run(steps)
+        e1.record()
+        torch.cuda.synchronize()
+        t_m = e0.elapsed_time(e1) / 1e3
+        out.update(merged_waters=total, merged_s=t_m, merged_water_steps_per_s=total * steps / t_m,
+                   batch_water_steps_per_s=total * steps / t_batch, batch_over_merged=t_m / t_batch)
         md.close()
         pot.close()
     if world > 1:
