@@ -344,12 +344,14 @@ __global__ void __launch_bounds__(kMxWarps * 32) k_pair_mixed(MixedArgs a)
 // charge only (the site layout of ElecLJ's groups for 3-site water,
 // src/eleclj.cpp:654-676).  The nine site pairs and the one LJ pair of a
 // group pair are straight-line code.  A warp owns one row group and walks its
-// list 32 entries at a time: each lane tests one partner's FP64 anchor
-// distance (anchors are requested one batch ahead, list indices two batches
-// ahead), and for an accepted partner writes the FP32 anchor displacement to
-// a 128-slot shared-memory ring and starts asynchronous copies (cp.async) of
-// the partner's 48-byte record into the same ring slot.  When 32 entries are
-// queued every lane evaluates one group pair from shared memory.  Per group
+// list 64 entries at a time: each lane tests two partners' anchor distances
+// (FP32, from cell-relative anchors; the next 64 anchors are requested one
+// step ahead, list indices two steps ahead), and for an accepted partner
+// writes the anchor displacement to a 128-slot shared-memory ring and starts
+// asynchronous copies (cp.async) of the partner's record (48 bytes, or the
+// 24 bytes of H offsets when every water has the same parameters) into the
+// same ring slot.  When 32 entries are queued every lane evaluates one group
+// pair from shared memory.  Per group
 // pair the kernel forms the FORCE on each row site (q E, plus LJ and switch
 // terms on O) and the pair energies, and converts those 11 values to fixed
 // point.
@@ -706,9 +708,12 @@ __device__ __forceinline__ void water_pair(const WaterArgs &a, const WaterRow &w
 }
 
 // One row group p, partners queued through the warp's ring: walks the row's
-// list (full rows, making the pruned ones, or the pruned rows); each lane
-// tests one partner's anchor distance, an accepted partner's displacement goes
-// to the ring and its record is copied there (cp.async); 32 queued pairs are
+// list (full rows, making the pruned ones, or the pruned rows) 64 entries per
+// step, two per lane, with the next step's 64 anchors already requested and
+// the list indices a step further ahead (a row has only a few steps, so each
+// step's load latency is what the walk waits on); each lane tests its
+// partners' anchor distances, an accepted partner's displacement goes to the
+// ring and its record is copied there (cp.async); 32 queued pairs are
 // evaluated at a time, one per lane.  qa, q0, q1, q2: the warp's ring.
 // Returns the row's first site.
 template <bool VIR, bool UNI>
@@ -733,53 +738,62 @@ __device__ __forceinline__ int water_row(const WaterArgs &a, int p, int lane, fl
   };
   // Entries past the row end read the row's own group (a valid address);
   // they are never accepted.
-  int jc = lane < cnt ? row[lane] : p;
-  int jn = lane + 32 < cnt ? row[lane + 32] : p;
-  float4 ac = a.anc32[jc];
+  int jc0 = lane < cnt ? row[lane] : p, jc1 = lane + 32 < cnt ? row[lane + 32] : p;
+  int jn0 = lane + 64 < cnt ? row[lane + 64] : p, jn1 = lane + 96 < cnt ? row[lane + 96] : p;
+  float4 ac0 = a.anc32[jc0], ac1 = a.anc32[jc1];
   int head = 0, qn = 0;  // ring entries [head, head + qn)
-  for (int base = 0; base < cnt; base += 32) {
-    const int e2 = base + 64 + lane;
-    const int jnn = e2 < cnt ? row[e2] : p;
-    const float4 an = a.anc32[jn];
-    const float3 d = cell_disp(a, w.ai, ac);
-    const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
-    const bool take = base + lane < cnt && r2 <= a.rhi2f;
-    if (make) {
-      const bool keep = base + lane < cnt && r2 <= a.rp2f;
-      const unsigned kb = __ballot_sync(0xffffffffu, keep);
-      if (keep)
-        prow[pn + __popc(kb & below)] = jc;
-      pn += __popc(kb);
-    }
-    const unsigned bal = __ballot_sync(0xffffffffu, take);
-    if (take) {
-      const int slot = (head + qn + __popc(bal & below)) & kMask;
-      qa[slot] = make_float4(d.x, d.y, d.z, r2);
-      const float4 *src = a.site + 3 * (size_t) jc;
-      cp_async16(&q0[slot], src);
-      if (UNI) {
-        cp_async8(&q1[slot], src + 1);  // the H z offsets; the charges are the arguments'
-      } else {
-        cp_async16(&q1[slot], src + 1);
-        cp_async16(&q2[slot], src + 2);
+  for (int base2 = 0; base2 < cnt; base2 += 64) {
+    const int e2 = base2 + 128 + lane;
+    const int jnn0 = e2 < cnt ? row[e2] : p, jnn1 = e2 + 32 < cnt ? row[e2 + 32] : p;
+    const float4 an0 = a.anc32[jn0], an1 = a.anc32[jn1];
+#pragma unroll
+    for (int hh = 0; hh < 2; hh++) {
+      const int base = base2 + 32 * hh;
+      const int jc = hh ? jc1 : jc0;
+      const float4 ac = hh ? ac1 : ac0;
+      const float3 d = cell_disp(a, w.ai, ac);
+      const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
+      const bool take = base + lane < cnt && r2 <= a.rhi2f;
+      if (make) {
+        const bool keep = base + lane < cnt && r2 <= a.rp2f;
+        const unsigned kb = __ballot_sync(0xffffffffu, keep);
+        if (keep)
+          prow[pn + __popc(kb & below)] = jc;
+        pn += __popc(kb);
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, take);
+      if (take) {
+        const int slot = (head + qn + __popc(bal & below)) & kMask;
+        qa[slot] = make_float4(d.x, d.y, d.z, r2);
+        const float4 *src = a.site + 3 * (size_t) jc;
+        cp_async16(&q0[slot], src);
+        if (UNI) {
+          cp_async8(&q1[slot], src + 1);  // the H z offsets; the charges are the arguments'
+        } else {
+          cp_async16(&q1[slot], src + 1);
+          cp_async16(&q2[slot], src + 2);
+        }
+      }
+      cp_async_commit();
+      // entries of earlier batches are evaluated one batch after their copies
+      // were started, so the copies are normally complete by then
+      const bool run = qn >= 32;
+      qn += __popc(bal);
+      if (run) {
+        cp_async_wait_prev();
+        __syncwarp();
+        compute((head + lane) & kMask);
+        __syncwarp();  // the slots are free again only after every lane has read them
+        head = (head + 32) & kMask;
+        qn -= 32;
       }
     }
-    cp_async_commit();
-    // entries of earlier batches are evaluated one batch after their copies
-    // were started, so the copies are normally complete by then
-    const bool run = qn >= 32;
-    qn += __popc(bal);
-    if (run) {
-      cp_async_wait_prev();
-      __syncwarp();
-      compute((head + lane) & kMask);
-      __syncwarp();  // the slots are free again only after every lane has read them
-      head = (head + 32) & kMask;
-      qn -= 32;
-    }
-    jc = jn;
-    jn = jnn;
-    ac = an;
+    jc0 = jn0;
+    jc1 = jn1;
+    jn0 = jnn0;
+    jn1 = jnn1;
+    ac0 = an0;
+    ac1 = an1;
   }
   cp_async_wait_all();
   __syncwarp();
