@@ -84,7 +84,10 @@ typedef struct mmnb_config {
   double smoothing_width;        /* 1 */
   double neighbor_list_width;    /* 0 -> 0.2 rc, clipped to 0.499 d - rc */
   double kspace_cutoff;          /* 5 (ordinary Ewald |n| cutoff) */
-  double ewald_screening;        /* -1 -> automatic; P3M needs an explicit value */
+  double ewald_screening;        /* -1 -> automatic: sqrt(pi kc / (rc d)) for the
+                                    k-sum; with P3M the value that minimises the
+                                    summed squares of the real-space and mesh error
+                                    estimates (src/pppm.c:666-716) */
   int use_p3m;                   /* 0 */
   double p3m_grid_spacing;       /* 0.5 */
   int p3m_assignment_order;      /* 3; 2..7 */
@@ -101,6 +104,9 @@ typedef struct mmnb_config {
                                     criterion (src/nbrlist.cpp:51-77); k > 0: also
                                     force a rebuild every k-th evaluation */
   int device;                    /* CUDA ordinal, -1 = current */
+  double p3m_grid_density;       /* -1; > 0: mesh spacing = minimum diameter /
+                                    cbrt(density * volume), and p3m_grid_spacing
+                                    must keep its default (src/eleclj.cpp:195-200) */
 } mmnb_config;
 
 /* Energies of the last evaluation (kcal/mol), as ElecLJ::write reports them
@@ -207,6 +213,14 @@ int mmnb_get_launches(mmnb_handle *h, long *launches);
 
 /* Derived settings: rc, neighbour-list width, eta, P3M mesh (0 if unused). */
 int mmnb_get_settings(mmnb_handle *h, double *rc, double *nlw, double *eta, int mesh[3]);
+
+/* The dimensionless RMS force error estimates ElecLJ::init reports
+   (src/eleclj.cpp:129-138, 225, 233-243): real space 2 / sqrt(rc / V^(1/3))
+   exp(-(rc eta)^2) (0 without real space), and reciprocal space -- with P3M the
+   mesh estimate p3m_init computes beside the influence function
+   (src/pppm.c:313-393), for the k-sum eta l / pi sqrt(8 / kc)
+   exp(-(pi kc / (eta l))^2), l = V^(1/3) (0 without k-space). */
+int mmnb_get_error_estimates(mmnb_handle *h, double *rspace, double *kspace);
 
 /* Stage timing with CUDA events on the handle's stream.  mmnb_set_timing
    clears the record and turns it on or off; while on, every evaluation

@@ -47,6 +47,7 @@ class MmnbConfig(ctypes.Structure):
         ("lj_1_4_scale_factor", ctypes.c_double),
         ("rebuild_interval", ctypes.c_int),
         ("device", ctypes.c_int),
+        ("p3m_grid_density", ctypes.c_double),
     ]
 
 
@@ -73,6 +74,7 @@ SIGNATURES = [
     ("mmnb_get_launches", ctypes.c_int, [_vp, _lp]),
     ("mmnb_check", ctypes.c_int, [_vp, _lp, _ip]),
     ("mmnb_get_settings", ctypes.c_int, [_vp, _dp, _dp, _dp, _ip]),
+    ("mmnb_get_error_estimates", ctypes.c_int, [_vp, _dp, _dp]),
     ("mmnb_set_timing", ctypes.c_int, [_vp, ctypes.c_int]),
     ("mmnb_get_timing", ctypes.c_int, [_vp, _dp, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
     ("mmnb_destroy", ctypes.c_int, [_vp]),

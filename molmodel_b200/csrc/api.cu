@@ -369,6 +369,76 @@ int setup_kspace(mmnb_handle *h)
   return MMNB_OK;
 }
 
+// p3m_optimize (src/pppm.c:666-716): the screening eta that minimises
+// chi_r^2 + chi_k^2, with chi_r = 2 / sqrt(rc / V^(1/3)) exp(-(rc eta)^2) the
+// real-space error estimate and chi_k the mesh's (p3m_init, here k_green at
+// that eta; a negative eta scores 1e8).  The reference runs GSL's one-variable
+// simplex (gsl_multimin_fminimizer_nmsimplex) from eta = 0.1 / spacing with a
+// step of 0.1 and stops it once the simplex size -- the mean distance of its
+// vertices from their centre -- is below 1e-4, or after 100 iterations.  The
+// same start, step, size test and iteration limit drive the Nelder-Mead moves
+// here as Lagarias, Reeds, M. Wright and P. Wright state them (SIAM J. Optim. 9
+// (1998) 112-147: reflection 1, expansion 2, contraction 1/2, shrink 1/2).
+// Both end within the size tolerance of the objective's minimum, not on the
+// same iterates.  The influence function is then made at the chosen eta (the
+// reference leaves the one of the last point its simplex evaluated).
+static int p3m_optimize_eta(mmnb_handle *h, double spacing)
+{
+  const double v13 = pow(h->volume, 1.0 / 3.0);
+  cudaError_t err = cudaSuccess;
+  auto objective = [&](double eta) {
+    if (eta < 0)
+      return 1e8;
+    const double chi_r = 2 / sqrt(h->rc / v13) * exp(-sq(h->rc * eta));
+    double chi_k = 0;
+    if (err == cudaSuccess)
+      err = launch_p3m_green(h, eta, &chi_k);
+    return sq(chi_r) + sq(chi_k);
+  };
+  double x[2] = {0.1 / spacing, 0.1 / spacing + 0.1};
+  double fx[2] = {objective(x[0]), objective(x[1])};
+  for (int it = 1; it <= 100 && err == cudaSuccess; it++) {
+    const int lo = fx[1] < fx[0] ? 1 : 0, hi = 1 - lo;
+    const double c = x[lo];  // centroid of the vertices other than the worst
+    const double xr = 2 * c - x[hi], fr = objective(xr);
+    bool shrink = false;
+    if (fr < fx[lo]) {
+      const double xe = 3 * c - 2 * x[hi], fe = objective(xe);
+      x[hi] = fe < fr ? xe : xr;
+      fx[hi] = fe < fr ? fe : fr;
+    } else if (fr < fx[hi]) {
+      const double xo = c + 0.5 * (xr - c), fo = objective(xo);
+      if (fo <= fr) {
+        x[hi] = xo;
+        fx[hi] = fo;
+      } else {
+        shrink = true;
+      }
+    } else {
+      const double xi = c + 0.5 * (x[hi] - c), fi = objective(xi);
+      if (fi < fx[hi]) {
+        x[hi] = xi;
+        fx[hi] = fi;
+      } else {
+        shrink = true;
+      }
+    }
+    if (shrink) {
+      x[hi] = c + 0.5 * (x[hi] - c);
+      fx[hi] = objective(x[hi]);
+    }
+    if (0.5 * fabs(x[1] - x[0]) < 1e-4)
+      break;
+  }
+  if (err != cudaSuccess)
+    return fail(h, MMNB_ERR_CUDA, std::string("P3M screening optimisation: ") + cudaGetErrorString(err));
+  h->eta = fx[1] < fx[0] ? x[1] : x[0];
+  h->eta_optimised = true;
+  if (!(h->eta > 0))
+    return fail(h, MMNB_ERR_ARG, "P3M screening optimisation did not find a positive eta");
+  return MMNB_OK;
+}
+
 int setup_p3m(mmnb_handle *h)
 {
   const mmnb_config &c = h->cfg;
@@ -378,12 +448,20 @@ int setup_p3m(mmnb_handle *h)
     return fail(h, MMNB_ERR_ARG, "p3m_alias_sum_limit must be 1..8");
   if (!(c.p3m_grid_spacing > 0))
     return fail(h, MMNB_ERR_ARG, "p3m_grid_spacing must be > 0");
+  // a grid density, when given, sets the spacing (src/eleclj.cpp:195-200)
+  double spacing = c.p3m_grid_spacing;
+  if (c.p3m_grid_density > 0) {
+    if (!almost_zero(spacing - 0.5))
+      return fail(h, MMNB_ERR_ARG, "only one of p3m_grid_spacing, p3m_grid_density should be specified");
+    spacing = h->min_diameter / cbrt(c.p3m_grid_density * h->volume);
+  }
   for (int d = 0; d < 3; d++)
-    h->mesh[d] = near_2357(floor(sqrt(sq(h->box.L[d])) / c.p3m_grid_spacing + 0.5));
+    h->mesh[d] = near_2357(floor(sqrt(sq(h->box.L[d])) / spacing + 0.5));
   const size_t nr = (size_t) h->mesh[0] * h->mesh[1] * h->mesh[2];
   const size_t nk = (size_t) h->mesh[0] * h->mesh[1] * (h->mesh[2] / 2 + 1);
   int s;
-  if ((s = dalloc(h, &h->d_green, nk)) || (s = dalloc(h, &h->d_kvec, 3 * nk)))
+  if ((s = dalloc(h, &h->d_green, nk)) || (s = dalloc(h, &h->d_kvec, 3 * nk)) ||
+      (s = dalloc(h, &h->d_chi_part, (nk + 127) / 128)))
     return s;
   if (c.precision == MMNB_MIXED) {
     if ((s = dalloc(h, &h->d_mesh_fx, nr)) || (s = dalloc(h, &h->d_mesh32, nr)) ||
@@ -408,13 +486,12 @@ int setup_p3m(mmnb_handle *h)
       if ((s = dalloc(h, &h->d_egrid, 3 * nr)) || (s = dalloc(h, &h->d_egridk, 3 * nk)))
         return s;
   }
-  CK(launch_p3m_green(h));
+  if (h->eta < 0 && (s = p3m_optimize_eta(h, spacing)))
+    return s;
+  CK(launch_p3m_green(h, h->eta, &h->p3m_chi));
   if (c.precision == MMNB_MIXED)
     CK(launch_green32(h));
-  double chi = 0;
-  CK(cudaMemcpyAsync(&chi, h->d_energy, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  h->p3m_chi = pow(1.0 / h->volume, 1.0 / 3.0) * sqrt(2 * fabs(chi));
   h->p3m = true;
   return MMNB_OK;
 }
@@ -442,7 +519,7 @@ void free_all(mmnb_handle *h)
                   h->d_mesh, h->d_meshk, h->d_green, h->d_kvec, h->d_egrid, h->d_egridk, h->d_mesh32,
                   h->d_meshk32, h->d_green32, h->d_egrid32, h->d_egridk32, h->d_mesh_fx, h->d_kint, h->d_kvecs, h->d_ak, h->d_skc,
                   h->mx.site, h->mx.par, h->mx.anchor, h->mx.anc32, h->mx.acc, h->mx.acck, h->d_wsum,
-                  h->d_bwd, h->d_gmesh, h->d_gmeshk};
+                  h->d_bwd, h->d_gmesh, h->d_gmeshk, h->d_chi_part};
   for (void *p : ptrs)
     if (p)
       cudaFree(p);
@@ -564,6 +641,7 @@ int mmnb_config_init(mmnb_config *c)
   c->lj_1_4_scale_factor = 1;
   c->rebuild_interval = 0;
   c->device = -1;
+  c->p3m_grid_density = -1;
   return MMNB_OK;
 }
 
@@ -632,16 +710,14 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
   h->rlo2 = sq(h->rc - c->smoothing_width);
   h->inv_sw = h->rhi2 > h->rlo2 ? 1.0 / (h->rhi2 - h->rlo2) : 0.0;
   // Ewald parameter (src/eleclj.cpp:189-239)
+  // (with P3M a negative value is resolved by setup_p3m, before the real-space
+  // table is made)
   h->eta = c->ewald_screening;
-  if (c->include_kspace && c->use_p3m) {
-    if (!(h->eta > 0))
-      return fail(h, MMNB_ERR_UNSUPPORTED,
-                  "P3M needs an explicit ewald_screening > 0 (eta optimisation is not provided)");
-  } else if (h->eta < 0) {
+  const bool p3m = c->include_kspace && c->use_p3m;
+  if (h->eta < 0 && !p3m)
     h->eta = sqrt((M_PI * c->kspace_cutoff) / (h->rc * h->min_diameter));
-  }
-  if (!(h->eta > 0))
-    return fail(h, MMNB_ERR_ARG, "ewald_screening must be > 0");
+  if (!(h->eta > 0) && !(p3m && h->eta < 0))
+    return fail(h, MMNB_ERR_ARG, "ewald_screening must be > 0, or negative for the automatic choice");
   // topology tables
   std::vector<std::pair<int, int>> ep, pp;
   for (int k = 0; k < nexcl; k++) {
@@ -755,17 +831,14 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
     return s;
   if ((s = alloc_rows(h, initial_rowcap(h))))
     return s;
+  if (c->include_kspace && c->use_p3m && (s = setup_p3m(h)))
+    return s;
   if ((s = setup_cheb(h)))
     return s;
-  if (c->include_kspace) {
-    if (c->use_p3m) {
-      if ((s = setup_p3m(h)))
-        return s;
-    } else {
-      h->kspace = true;
-      if ((s = setup_kspace(h)))
-        return s;
-    }
+  if (c->include_kspace && !c->use_p3m) {
+    h->kspace = true;
+    if ((s = setup_kspace(h)))
+      return s;
   }
   return MMNB_OK;
 }
@@ -1395,6 +1468,22 @@ int mmnb_get_settings(mmnb_handle *h, double *rc, double *nlw, double *eta, int 
   if (mesh)
     for (int d = 0; d < 3; d++)
       mesh[d] = h->mesh[d];
+  return MMNB_OK;
+}
+
+int mmnb_get_error_estimates(mmnb_handle *h, double *rspace, double *kspace)
+{
+  if (!h)
+    return MMNB_ERR_ARG;
+  const double l = cbrt(h->volume);
+  if (rspace)
+    *rspace = h->cfg.include_rspace ? 2 / sqrt(h->rc / l) * exp(-sq(h->rc * h->eta)) : 0.0;
+  if (kspace) {
+    const double kc = h->cfg.kspace_cutoff;
+    *kspace = !h->cfg.include_kspace ? 0.0
+              : h->p3m               ? h->p3m_chi
+                                     : h->eta * l / M_PI * sqrt(8 / kc) * exp(-sq(M_PI * kc / (h->eta * l)));
+  }
   return MMNB_OK;
 }
 

@@ -238,7 +238,9 @@ struct mmnb_handle {
   double *d_kvec = nullptr;          // 3 per k-point (ik differentiation)
   double *d_egrid = nullptr;         // 3 real meshes (ik)
   cufftDoubleComplex *d_egridk = nullptr;
-  double p3m_chi = 0;
+  double *d_chi_part = nullptr;      // per-block partials of the mesh error sum
+  double p3m_chi = 0;                // the mesh's dimensionless RMS force error estimate
+  bool eta_optimised = false;        // eta chosen by p3m_optimize's criterion
   // mixed-precision P3M
   cufftHandle plan_r2c32 = 0, plan_c2r32 = 0;
   float *d_mesh32 = nullptr;
@@ -295,7 +297,7 @@ cudaError_t launch_rspace_water(mmnb_handle *h);
 cudaError_t launch_sort_water64(mmnb_handle *h, const double *d_r);
 cudaError_t launch_rspace_water64(mmnb_handle *h);
 cudaError_t launch_exclusions(mmnb_handle *h, const double *d_r);
-cudaError_t launch_p3m_green(mmnb_handle *h);
+cudaError_t launch_p3m_green(mmnb_handle *h, double eta, double *chi);
 // stage bit 1: spread + FFT round trip, bit 2: gather
 cudaError_t launch_p3m_fp64(mmnb_handle *h, const double *d_r, int stage);
 // FP64 meshes and plans of the adjoint's dipole solve: spread/spreadk hold one

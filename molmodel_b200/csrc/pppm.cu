@@ -89,6 +89,8 @@ __device__ __forceinline__ int wrap_idx(int i, int n)
 
 // ---- influence function -----------------------------------------------------
 
+constexpr int kGreenThreads = 128;
+
 struct GreenArgs {
   int n[3];
   int nalias, order, ik;
@@ -103,12 +105,10 @@ __device__ __forceinline__ double sincpi_d(double x)
   return fabs(y) < 1e-16 ? 1 - y * y / 6 : sin(y) / y;
 }
 
-__global__ void k_green(GreenArgs a)
+// G(k) of one half-mesh point g (and its k-vector); returns the point's term of
+// the RMS force error sum, sum_p g_p^2 k_p^2 - numerator^2 / denominator
+__device__ double green_point(const GreenArgs &a, long g, int nx, int ny, int nz, int nzh)
 {
-  const int nx = a.n[0], ny = a.n[1], nz = a.n[2], nzh = nz / 2 + 1;
-  const long g = (long) blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= (long) nx * ny * nzh)
-    return;
   const int iz = (int) (g % nzh);
   const int iy = (int) ((g / nzh) % ny);
   const int ix = (int) (g / ((long) nzh * ny));
@@ -127,7 +127,7 @@ __global__ void k_green(GreenArgs a)
   }
   if (ix == 0 && iy == 0 && iz == 0) {
     a.green[g] = 0;
-    return;
+    return 0.0;
   }
   const double k2 = kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2];
   constexpr int kMaxAlias = 8;
@@ -168,11 +168,37 @@ __global__ void k_green(GreenArgs a)
   const double den = a.ik ? d1 * d1 * k2 : d1 * d2;
   a.green[g] = a.inv_v * num / den;
   chi -= num * num / den;
-  if (a.chi)
-    atomicAdd(a.chi, chi);
+  return chi;
 }
 
-cudaError_t launch_p3m_green(mmnb_handle *h)
+__global__ void k_green(GreenArgs a)
+{
+  const int nx = a.n[0], ny = a.n[1], nz = a.n[2], nzh = nz / 2 + 1;
+  const long g = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  const double chi = g < (long) nx * ny * nzh ? green_point(a, g, nx, ny, nz, nzh) : 0.0;
+  if (!a.chi)
+    return;
+  // chi of this block's points, summed in a fixed order (one partial per block)
+  __shared__ double part[kGreenThreads / 32];
+  double v = chi;
+  for (int o = 16; o > 0; o >>= 1)
+    v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0)
+    part[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < kGreenThreads / 32; w++)
+      t += part[w];
+    a.chi[blockIdx.x] = t;
+  }
+}
+
+// G(k) and the k-vectors of the handle's mesh at screening eta (p3m_init,
+// src/pppm.c:313-393); with chi non-null also the reference's dimensionless RMS
+// force error estimate V^(-1/3) sqrt(2 |sum|), its per-block partials added in
+// block order on the host so that the value does not depend on scheduling
+cudaError_t launch_p3m_green(mmnb_handle *h, double eta, double *chi)
 {
   GreenArgs a;
   for (int d = 0; d < 3; d++)
@@ -186,14 +212,27 @@ cudaError_t launch_p3m_green(mmnb_handle *h)
   for (int d = 0; d < 3; d++)
     a.rec[4 * d] = 2 * M_PI * (1.0 / h->box.L[d]);
   a.inv_v = 1.0 / h->volume;
-  a.inv_4eta2 = 1 / ((2 * h->eta) * (2 * h->eta));
+  a.inv_4eta2 = 1 / ((2 * eta) * (2 * eta));
   a.green = h->d_green;
   a.kvec = h->d_kvec;
-  a.chi = h->d_energy;  // scratch: reduced chi lands in d_energy[0]
+  a.chi = chi ? h->d_chi_part : nullptr;
   const long nk = (long) h->mesh[0] * h->mesh[1] * (h->mesh[2] / 2 + 1);
-  cudaMemsetAsync(h->d_energy, 0, sizeof(double), h->stream);
-  k_green<<<div_up(nk, 128), 128, 0, h->stream>>>(a);
-  return cudaGetLastError();
+  const int nblock = (int) div_up(nk, kGreenThreads);
+  k_green<<<nblock, kGreenThreads, 0, h->stream>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !chi)
+    return e;
+  std::vector<double> part(nblock);
+  e = cudaMemcpyAsync(part.data(), h->d_chi_part, sizeof(double) * nblock, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess)
+    return e;
+  double sum = 0;
+  for (int b = 0; b < nblock; b++)
+    sum += part[b];
+  *chi = pow(a.inv_v, 1.0 / 3.0) * sqrt(2 * fabs(sum));
+  return cudaSuccess;
 }
 
 // ---- FP64 spread / gather -----------------------------------------------------

@@ -38,7 +38,7 @@ class ElecLJ:
 
     def __init__(self, precision="fp64", rspace_cutoff=0.0, smoothing_width=1.0,
                  neighbor_list_width=0.0, kspace_cutoff=5.0, ewald_screening=-1.0,
-                 use_p3m=False, p3m_grid_spacing=0.5, p3m_assignment_order=3,
+                 use_p3m=False, p3m_grid_spacing=0.5, p3m_grid_density=-1.0, p3m_assignment_order=3,
                  p3m_alias_sum_limit=2, p3m_ik_differentiate=False,
                  include_lj_correction=True, geometric_combining_for_sigma=False,
                  include_rspace=True, include_kspace=True, include_self=True,
@@ -52,6 +52,7 @@ class ElecLJ:
         self.ewald_screening = ewald_screening
         self.use_p3m = use_p3m
         self.p3m_grid_spacing = p3m_grid_spacing
+        self.p3m_grid_density = p3m_grid_density
         self.p3m_assignment_order = p3m_assignment_order
         self.p3m_alias_sum_limit = p3m_alias_sum_limit
         self.p3m_ik_differentiate = p3m_ik_differentiate
@@ -77,7 +78,7 @@ class ElecLJ:
         b = np.broadcast_to(np.asarray(box, dtype=np.float64), (3,))
         c.box = (ctypes.c_double * 3)(*b)
         for name in ("rspace_cutoff", "smoothing_width", "neighbor_list_width", "kspace_cutoff",
-                     "ewald_screening", "p3m_grid_spacing", "elec_1_4_scale_factor",
+                     "ewald_screening", "p3m_grid_spacing", "p3m_grid_density", "elec_1_4_scale_factor",
                      "lj_1_4_scale_factor"):
             setattr(c, name, float(getattr(self, name)))
         for name in ("use_p3m", "p3m_assignment_order", "p3m_alias_sum_limit", "p3m_ik_differentiate",
@@ -287,6 +288,13 @@ class ElecLJ:
         check(load().mmnb_get_settings(self._h, ctypes.byref(rc), ctypes.byref(nlw), ctypes.byref(eta),
                                        _i(mesh)), self._h)
         return dict(rc=rc.value, nlw=nlw.value, eta=eta.value, mesh=tuple(int(x) for x in mesh))
+
+    def error_estimates(self):
+        """(real space, reciprocal space) dimensionless RMS force error estimates,
+        the two figures ElecLJ::init reports (src/eleclj.cpp:225, 233-243)."""
+        rs, ks = ctypes.c_double(), ctypes.c_double()
+        check(load().mmnb_get_error_estimates(self._h, ctypes.byref(rs), ctypes.byref(ks)), self._h)
+        return rs.value, ks.value
 
     def set_timing(self, on=True):
         check(load().mmnb_set_timing(self._h, int(on)), self._h)

@@ -173,6 +173,51 @@ class OracleLib:
         self.lib.orc_p3m_delete(h)
         return phi, evec, tuple(int(x) for x in ngrid), chi.value
 
+    def p3m_chi(self, latv, spacing, order, eta, nalias=2, ik=False):
+        """p3m_init's dimensionless RMS force error estimate (src/pppm.c:313-393)
+        for the mesh p3m_new picks (src/pppm.c:395-447); returns (chi, mesh)."""
+        ngrid = np.zeros(3, dtype=np.int32)
+        chi = ctypes.c_double()
+        h = self.lib.orc_p3m_new(0, _d(_f64(latv)), spacing, nalias, int(ik), order, eta, _i(ngrid),
+                                 ctypes.byref(chi))
+        self.lib.orc_p3m_delete(h)
+        return chi.value, tuple(int(x) for x in ngrid)
+
+    def p3m_optimize_objective(self, latv, spacing, order, rc, eta, nalias=2, ik=False):
+        """p3m_optimize_help (src/pppm.c:672-681): chi_r^2 + chi_k^2 at eta, 1e8
+        for a negative eta."""
+        if eta < 0:
+            return 1e8
+        v = abs(np.linalg.det(_f64(latv).reshape(3, 3)))
+        chi_r = 2 / np.sqrt(rc / v ** (1.0 / 3.0)) * np.exp(-(rc * eta) ** 2)
+        return chi_r ** 2 + self.p3m_chi(latv, spacing, order, eta, nalias, ik)[0] ** 2
+
+    def p3m_optimize(self, latv, spacing, order, rc, nalias=2, ik=False, tol=1e-9):
+        """The minimiser of p3m_optimize's objective (src/pppm.c:682-716).  The
+        reference finds it with GSL's simplex (gsl_multimin_fminimizer_nmsimplex,
+        size tolerance 1e-4), which the oracle build does not have; this
+        restatement brackets the minimum on a coarse scan of the same objective
+        and closes the bracket by golden-section search to ``tol``, so it gives the
+        point the simplex converges to, not the simplex's own last vertex."""
+        f = lambda e: self.p3m_optimize_objective(latv, spacing, order, rc, e, nalias, ik)
+        grid = np.linspace(0.02, 1.5, 75)
+        vals = [f(e) for e in grid]
+        k = int(np.argmin(vals))
+        a, b = grid[max(k - 1, 0)], grid[min(k + 1, len(grid) - 1)]
+        g = (np.sqrt(5) - 1) / 2
+        c, d = b - g * (b - a), a + g * (b - a)
+        fc, fd = f(c), f(d)
+        while b - a > tol:
+            if fc < fd:
+                b, d, fd = d, c, fc
+                c = b - g * (b - a)
+                fc = f(c)
+            else:
+                a, c, fc = c, d, fd
+                d = a + g * (b - a)
+                fd = f(d)
+        return 0.5 * (a + b)
+
     def water_constrain_positions(self, r0, r, v, mass3, dt, r_oh=1.0, angle_deg=109.47, tol=1e-12,
                                   maxit=10000):
         """ConstraintGroup::constrain_positions (src/constraint.cpp:295-335) on every

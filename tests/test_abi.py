@@ -4,6 +4,7 @@ import ctypes
 import glob
 import os
 import re
+import subprocess
 
 import numpy as np
 
@@ -42,6 +43,22 @@ def test_config_defaults_are_the_references():
     assert (c.p3m_assignment_order, c.p3m_alias_sum_limit, c.p3m_ik_differentiate) == (3, 2, 0)
     assert c.include_lj_correction == 1 and c.geometric_combining_for_sigma == 0
     assert (c.include_rspace, c.include_kspace, c.include_self) == (1, 1, 1)
+    assert c.p3m_grid_density == -1
+
+
+def test_config_mirror_has_the_headers_layout(tmp_path):
+    """Every field of the ctypes mirror sits at the offset the C compiler gives
+    it in include/mmnb.h, and the two structs have one size."""
+    fields = [f for f, _ in _lib.MmnbConfig._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text("#include <stdio.h>\n#include <stddef.h>\n#include \"mmnb.h\"\nint main(void) {\n"
+                   + "".join('  printf("%%zu\\n", offsetof(mmnb_config, %s));\n' % f for f in fields)
+                   + '  printf("%zu\\n", sizeof(mmnb_config));\n  return 0;\n}\n')
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    want = [getattr(_lib.MmnbConfig, f).offset for f in fields] + [ctypes.sizeof(_lib.MmnbConfig)]
+    assert got == want
 
 
 def test_chebyshev_table_is_the_oracles_bitwise():

@@ -93,6 +93,26 @@ def test_port_vs_reference_p3m_orders(order):
 
 
 @ref_only
+@pytest.mark.parametrize("box,spacing,order,nalias,ik", [
+    ((18.6, 18.6, 18.6), 0.5, 5, 2, False),
+    ((15.5, 17.0, 16.2), 0.8, 3, 1, False),
+    ((15.5, 15.5, 15.5), 0.8, 4, 2, True),
+])
+def test_port_vs_reference_p3m_error_estimate(box, spacing, order, nalias, ik):
+    """p3m_init's RMS force error estimate (src/pppm.c:313-393), the objective
+    p3m_optimize minimises (src/pppm.c:672-681): the port gives the reference's
+    value and mesh bitwise at several screenings."""
+    latv = np.diag(box)
+    for eta in (0.2, 0.3, 0.45):
+        a = reference().p3m_chi(latv, spacing, order, eta, nalias, ik)
+        b = port().p3m_chi(latv, spacing, order, eta, nalias, ik)
+        assert a == b
+        assert reference().p3m_optimize_objective(latv, spacing, order, 7.0, eta, nalias, ik) == \
+            port().p3m_optimize_objective(latv, spacing, order, 7.0, eta, nalias, ik)
+    assert port().p3m_optimize_objective(latv, spacing, order, 7.0, -0.1) == 1e8
+
+
+@ref_only
 def test_port_vs_reference_orthorhombic_and_list():
     wb = water_box(6, seed=9)
     stretch = np.array([1.0, 1.08, 0.96])
