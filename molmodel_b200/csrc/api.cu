@@ -2,6 +2,8 @@
 // (src/eleclj.cpp:140-265), and the per-evaluation launch sequence that
 // mirrors ElecLJ::add_to_energy_and_forces (src/eleclj.cpp:785-807).
 
+#include <atomic>
+
 #include "mmnb_internal.cuh"
 
 #include <algorithm>
@@ -508,6 +510,20 @@ void free_all(mmnb_handle *h)
     cudaEventDestroy(h->ev_flags);
     h->ev_flags = nullptr;
   }
+  for (cudaEvent_t &ev : h->ev_in)
+    if (ev) {
+      cudaEventDestroy(ev);
+      ev = nullptr;
+    }
+  if (h->ev_free) {
+    cudaEventDestroy(h->ev_free);
+    h->ev_free = nullptr;
+  }
+  if (h->copy_in) {
+    cudaStreamSynchronize(h->copy_in);
+    cudaStreamDestroy(h->copy_in);
+    h->copy_in = nullptr;
+  }
   void *ptrs[] = {h->d_group, h->d_excl_ptr, h->d_excl_idx, h->d_p14_ptr, h->d_p14_idx, h->d_gexcl_ptr,
                   h->d_gexcl_idx, h->d_mask, h->d_q, h->d_sig, h->d_eps, h->d_rscreen, h->d_cheb, h->d_cheb_w, h->d_cheb_d, h->d_lj_row, h->d_lj_row_part,
                   h->d_vir_part, h->d_vir_row, h->d_vir_mol, h->d_vir_molw, h->d_vir_mass,
@@ -539,6 +555,8 @@ void free_all(mmnb_handle *h)
     cudaFreeHost(h->h_f);
   if (h->h_out)
     cudaFreeHost(h->h_out);
+  if (h->h_status)
+    cudaFreeHost(h->h_status);
   if (h->plan_r2c)
     cufftDestroy(h->plan_r2c);
   if (h->plan_c2r)
@@ -804,7 +822,7 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
       (s = dalloc(h, &h->d_ljf, 3 * (size_t) nsite)) || (s = dalloc(h, &h->d_lj_part, nlj)) ||
       (s = dalloc(h, &h->d_lj_row, ngroup)) || (s = dalloc(h, &h->d_vir_part, nlj)) ||
       (s = dalloc(h, &h->d_vir_row, ngroup)) ||
-      (s = dalloc(h, &h->d_elec_part, h->elec_blocks)) || (s = dalloc(h, &h->d_lj_row_part, h->elec_blocks)) || (s = dalloc(h, &h->d_energy, 8)) ||
+      (s = dalloc(h, &h->d_elec_part, h->elec_blocks)) || (s = dalloc(h, &h->d_lj_row_part, h->elec_blocks)) || (s = dalloc(h, &h->d_energy, 16)) ||
       (s = dalloc(h, &h->d_r, 3 * (size_t) nsite)) || (s = dalloc(h, &h->d_f, 3 * (size_t) nsite)) ||
       (s = dalloc(h, &h->d_wsum, 8)))
     return s;
@@ -820,6 +838,9 @@ static int create_impl(mmnb_handle *h, const mmnb_config *c, int nsite, int ngro
   }
   CK(cudaMallocHost((void **) &h->h_f, sizeof(double) * 3 * (size_t) nsite));
   CK(cudaMallocHost((void **) &h->h_out, sizeof(double) * 16));
+  CK(cudaHostAlloc((void **) &h->h_status, sizeof(double) * mmnb_handle::kStatusDoubles, cudaHostAllocMapped));
+  CK(cudaHostGetDevicePointer((void **) &h->d_status, h->h_status, 0));
+  memset(h->h_status, 0, sizeof(double) * mmnb_handle::kStatusDoubles);
   if ((s = setup_cells(h)))
     return s;
   // the rigid-water kernel's rows pruned to rc + width / 3: rebuilt (by that
@@ -970,6 +991,14 @@ int mmnb_set_params(mmnb_handle *h, const int *site_mask, const double *q, const
   return MMNB_OK;
 }
 
+// sites [lo, hi) of the host call's c-th positions piece
+static void in_chunk_sites(const mmnb_handle *h, int c, int &lo, int &hi)
+{
+  const int n = mmnb_handle::kInChunks;
+  lo = (int) ((long) h->nsite * c / n);
+  hi = (int) ((long) h->nsite * (c + 1) / n);
+}
+
 int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *d_energy)
 {
   if (!h || !d_r)
@@ -1003,26 +1032,42 @@ int mmnb_compute_device(mmnb_handle *h, const double *d_r, double *d_f, double *
   // so it joins the mesh work; the FP64 interpolation adds into the site
   // arrays the pair kernels write and waits for them
   const int mesh_stages = mixed ? 3 : 1;
-  if (p3m && !side)
-    CK(mixed ? launch_p3m_mixed(h, d_r, mesh_stages) : launch_p3m_fp64(h, d_r, mesh_stages));
   if (side) {
     cudaStream_t main = h->stream;
     CK(cudaEventRecord(h->ev_fork, main));
     CK(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
     h->stream = h->side;
     cudaError_t e = cudaSuccess;
-    if (excl_side) {
+    int stages = mesh_stages;
+    if (h->in_chunks) {
+      // the host call's positions arrive in pieces: each piece's charges are
+      // assigned as it lands (mixed form), the rest follows the last piece
+      for (int c = 0; c < mmnb_handle::kInChunks && e == cudaSuccess; c++) {
+        e = cudaStreamWaitEvent(h->side, h->ev_in[c], cudaEventWaitExternal);
+        int lo, hi;
+        in_chunk_sites(h, c, lo, hi);
+        if (e == cudaSuccess && mixed)
+          e = launch_spread_mixed_range(h, d_r, lo, hi);
+      }
+      if (mixed)
+        stages |= 4;
+    }
+    if (excl_side && e == cudaSuccess) {
       e = launch_exclusions(h, d_r);
       timing_mark(h, "rspace_excl");
     }
     if (e == cudaSuccess)
-      e = mixed ? launch_p3m_mixed(h, d_r, mesh_stages) : launch_p3m_fp64(h, d_r, mesh_stages);
+      e = mixed ? launch_p3m_mixed(h, d_r, stages) : launch_p3m_fp64(h, d_r, stages);
     h->stream = main;
     CK(e);
     CK(cudaEventRecord(h->ev_join, h->side));
     if (h->timing.on)
       CK(cudaStreamWaitEvent(main, h->ev_join, 0));
   }
+  if (h->in_chunks)
+    CK(cudaStreamWaitEvent(h->stream, h->ev_in[mmnb_handle::kInChunks - 1], cudaEventWaitExternal));
+  if (p3m && !side)
+    CK(mixed ? launch_p3m_mixed(h, d_r, mesh_stages) : launch_p3m_fp64(h, d_r, mesh_stages));
   CK(launch_list_check(h, d_r, h->force_rebuild_next));
   CK(launch_list_rebuild(h));
   timing_mark(h, "nbrlist");
@@ -1160,21 +1205,47 @@ static int compute_host(mmnb_handle *h, const double *r, double *f, double *u, m
     for (cudaEvent_t &ev : h->ev_chunk)
       CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   }
+  volatile unsigned long long *ready =
+      reinterpret_cast<volatile unsigned long long *>(h->h_status) + mmnb_handle::kStatusReady;
   for (int attempt = 0; attempt < 2; attempt++) {
-    CK(cudaMemcpyAsync(h->d_r, r, sizeof(double) * n3, cudaMemcpyHostToDevice, h->stream));
+    *ready = 0ull;  // k_finalize sets it once this evaluation's status is in place
     // after the first call, a plain evaluation replays the handle's own graph
     // (zeroing, list check/rebuild, pair and mesh kernels, finalize)
     const bool graph =
         !h->first && !(phi || evec || keep) && !h->timing.on && !h->force_rebuild_next && !h->want_virial;
+    if (graph) {
+      // the positions in pieces on the copy stream (once the handle's stream
+      // is done with d_r); the graph waits for each piece where it needs it
+      if (!h->copy_in) {
+        CK(cudaStreamCreateWithFlags(&h->copy_in, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&h->ev_free, cudaEventDisableTiming));
+        for (cudaEvent_t &ev : h->ev_in)
+          CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      }
+      CK(cudaEventRecord(h->ev_free, h->stream));
+      CK(cudaStreamWaitEvent(h->copy_in, h->ev_free, 0));
+      for (int c = 0; c < mmnb_handle::kInChunks; c++) {
+        int lo, hi;
+        in_chunk_sites(h, c, lo, hi);
+        if (hi > lo)
+          CK(cudaMemcpyAsync(h->d_r + 3 * (size_t) lo, r + 3 * (size_t) lo, sizeof(double) * 3 * (hi - lo),
+                             cudaMemcpyHostToDevice, h->copy_in));
+        CK(cudaEventRecord(h->ev_in[c], h->copy_in));
+      }
+    } else {
+      CK(cudaMemcpyAsync(h->d_r, r, sizeof(double) * n3, cudaMemcpyHostToDevice, h->stream));
+    }
     if (graph && !h->hgraph_exec) {
       CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
       h->capturing = true;
+      h->in_chunks = true;
       const long ev = h->evals, ln = h->launches;
       cudaError_t ce = cudaMemsetAsync(h->d_f, 0, sizeof(double) * n3, h->stream);
       if (ce == cudaSuccess)
         ce = cudaMemsetAsync(h->d_flags + kFlagOverflow, 0, sizeof(int), h->stream);
       const int s = ce == cudaSuccess ? mmnb_compute_device(h, h->d_r, h->d_f, h->d_energy) : MMNB_ERR_CUDA;
       h->capturing = false;
+      h->in_chunks = false;
       cudaGraph_t g = nullptr;
       const cudaError_t ec = cudaStreamEndCapture(h->stream, &g);
       h->evals = ev;
@@ -1203,10 +1274,10 @@ static int compute_host(mmnb_handle *h, const double *r, double *f, double *u, m
       if (s)
         return s;
     }
-    // flags first (a row overflow means evaluating again), then the forces in
-    // chunks, each added to f while the next one is in flight
-    CK(cudaMemcpyAsync(h->h_flags, h->d_flags, sizeof(int) * kFlagCount, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(h->h_out, h->d_energy, sizeof(double) * 4, cudaMemcpyDeviceToHost, h->stream));
+    // the energies and flags come through the mapped status block (a row
+    // overflow means evaluating again); the forces follow in chunks, each
+    // added to f while the next one is in flight
+    static_assert(4 + (kFlagCount + 1) / 2 <= mmnb_handle::kStatusReady, "status block");
     CK(cudaEventRecord(h->ev_flags, h->stream));
     const int nch = mmnb_handle::kChunks;
     const size_t per = (n3 + nch - 1) / nch;
@@ -1220,7 +1291,27 @@ static int compute_host(mmnb_handle *h, const double *r, double *f, double *u, m
       CK(cudaMemcpyAsync(phi, h->d_phi, sizeof(double) * h->nsite, cudaMemcpyDeviceToHost, h->stream));
     if (evec)
       CK(cudaMemcpyAsync(evec, h->d_evec, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaEventSynchronize(h->ev_flags));
+    // while the device works: drop the staging buffer's lines from the host
+    // caches (the last call's adds read them), so that the copies into it do
+    // not have to snoop them
+    if (f && n3 * sizeof(double) >= (1u << 20))
+      evict_host_lines(h->h_f, sizeof(double) * n3);
+    // the status block's ready word; the event only tells a failed
+    // evaluation apart
+    for (unsigned it = 1; *ready == 0ull; it++) {
+      if ((it & 255u) != 0)
+        continue;
+      const cudaError_t q = cudaEventQuery(h->ev_flags);
+      if (q == cudaErrorNotReady)
+        continue;
+      if (q != cudaSuccess)
+        return fail(h, MMNB_ERR_CUDA, std::string("evaluation: ") + cudaGetErrorString(q));
+      if (*ready == 0ull)
+        return fail(h, MMNB_ERR_CUDA, "the evaluation ended without writing its status");
+    }
+    std::atomic_thread_fence(std::memory_order_acquire);
+    memcpy(h->h_out, h->h_status, 4 * sizeof(double));
+    memcpy(h->h_flags, h->h_status + 4, sizeof(int) * kFlagCount);
     h->rebuilds = h->h_flags[5];
     if (h->h_flags[kFlagError]) {
       // a device-side check failed (non-finite site coordinates): nothing is

@@ -30,6 +30,8 @@ struct FinArgs {
   const unsigned long long *wsum;     // water kernel's fixed-point pair energies, or null
   unsigned long long *counter;        // finished-block counter, left at 0
   int *flags;                         // list flags: counts evaluations finished on cut rows
+  double *status;                     // or null: the host call's mapped status block
+                                      // (energies, flags, ready word)
   double tail;
   double *energy;
 };
@@ -146,6 +148,19 @@ __global__ void __launch_bounds__(kFinThreads) k_finalize(FinArgs a)
     *a.counter = 0ull;
     if (a.flags[kFlagListTrunc])
       a.flags[kFlagTruncEvals] += 1;
+    if (a.status) {
+      // over the bus to the waiting host: the block first, the ready word last
+      volatile double *st = a.status;
+      st[0] = elec;
+      st[1] = ljt;
+      st[2] = a.tail;
+      st[3] = elec + ljt;
+      volatile int *fl = reinterpret_cast<volatile int *>(a.status + 4);
+      for (int k = 0; k < kFlagCount; k++)
+        fl[k] = a.flags[k];
+      __threadfence_system();
+      reinterpret_cast<volatile unsigned long long *>(a.status)[mmnb_handle::kStatusReady] = 1ull;
+    }
   }
 }
 
@@ -180,6 +195,7 @@ cudaError_t launch_finalize(mmnb_handle *h, double *d_f, double *d_energy)
   a.flags = h->d_flags;
   a.tail = h->cfg.include_lj_correction ? h->lj_correction : 0.0;
   a.energy = d_energy;
+  a.status = d_energy == h->d_energy ? h->d_status : nullptr;
   k_finalize<<<h->elec_blocks, kFinThreads, 0, h->stream>>>(a);
   h->launches += 1;
   return cudaGetLastError();

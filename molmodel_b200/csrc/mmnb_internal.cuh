@@ -273,9 +273,25 @@ struct mmnb_handle {
   cudaGraphExec_t hgraph_exec = nullptr;
   long host_launch_per_eval = 0;
   // the host call copies the forces back in chunks and adds each as it lands
-  static constexpr int kChunks = 4;
+  static constexpr int kChunks = 2;
   cudaEvent_t ev_chunk[kChunks] = {};
   cudaEvent_t ev_flags = nullptr;
+  // ... and, replaying its graph, copies the positions in kInChunks pieces on
+  // a stream of its own: the graph's mesh branch assigns the charges of each
+  // piece as it lands (mixed form), everything else waits for the last piece
+  static constexpr int kInChunks = 2;
+  cudaStream_t copy_in = nullptr;
+  cudaEvent_t ev_in[kInChunks] = {};
+  cudaEvent_t ev_free = nullptr;  // the handle's stream has let go of d_r
+  bool in_chunks = false;         // set while that graph is captured
+  // the host call's status block in mapped pinned memory: k_finalize writes
+  // the energies [0, 4), the flags (ints, from double 4 on) and then, after a
+  // system-wide fence, the ready word; the host spins on that word instead of
+  // copying the block back after the evaluation
+  static constexpr int kStatusDoubles = 16;
+  static constexpr int kStatusReady = 15;  // double slot of the ready word
+  double *h_status = nullptr;
+  double *d_status = nullptr;  // its device alias
   bool capturing = false;
 };
 
@@ -315,6 +331,13 @@ cudaError_t launch_p3m_dipole_fp64(mmnb_handle *h, const double *d_r, const doub
 cudaError_t launch_kspace_dipole(mmnb_handle *h, const double *d_r, const double *d_g, double *d_skd,
                                  double *d_psi);
 cudaError_t launch_p3m_mixed(mmnb_handle *h, const double *d_r, int stage);
+// write back and drop [p, p + bytes) from the host cores' caches (hostmem.cpp)
+void evict_host_lines(const void *p, size_t bytes);
+
+// the mixed charge assignment of sites [lo, hi) alone; stage bit 4 of
+// launch_p3m_mixed then skips it (the mesh words are integer sums, so the
+// pieces give the mesh of one launch over all sites, bit for bit)
+cudaError_t launch_spread_mixed_range(mmnb_handle *h, const double *d_r, int lo, int hi);
 cudaError_t launch_green32(mmnb_handle *h);
 cudaError_t launch_kspace(mmnb_handle *h, const double *d_r);
 cudaError_t launch_finalize(mmnb_handle *h, double *d_f, double *d_energy);

@@ -884,6 +884,30 @@ cudaError_t launch_green32(mmnb_handle *h)
   return cudaGetLastError();
 }
 
+// charge assignment of sites [lo, hi) into the fixed-point mesh, in the
+// layout the handle's tuning picks
+template <int P>
+static void spread_mixed_p(mmnb_handle *h, const MeshArgs &m, const double *d_r, int lo, int hi)
+{
+  const int n = hi - lo;
+  if (n <= 0)
+    return;
+  const double *r = d_r + 3 * (size_t) lo;
+  const double *q = h->d_q + lo;
+  const int *mask = h->d_mask + lo;
+  if (h->tune.spread_planes == 2)
+    k_spread_mixed_zlanes<P><<<div_up(div_up(n, 32 / P) * 32, 128), 128, 0, h->stream>>>(m, r, q, mask, n,
+                                                                                       h->d_mesh_fx);
+  else if (h->tune.spread_planes)
+    k_spread_mixed_planes<P><<<div_up(n * P, 128), 128, 0, h->stream>>>(m, r, q, mask, n, h->d_mesh_fx);
+  else
+    k_spread_mixed<P><<<div_up(n, 128), 128, 0, h->stream>>>(m, r, q, mask, n, h->d_mesh_fx);
+  h->launches += 1;
+}
+
+// stage bits: 1 charge assignment and transforms, 2 interpolation, 4 (with 1)
+// the transforms without the assignment (done piecewise by
+// launch_spread_mixed_range)
 template <int P>
 static cudaError_t p3m_mixed_p(mmnb_handle *h, const double *d_r, int stage)
 {
@@ -891,15 +915,8 @@ static cudaError_t p3m_mixed_p(mmnb_handle *h, const double *d_r, int stage)
   const size_t nr = (size_t) h->mesh[0] * h->mesh[1] * h->mesh[2];
   const long nk = (long) h->mesh[0] * h->mesh[1] * (h->mesh[2] / 2 + 1);
   if (stage & 1) {
-    if (h->tune.spread_planes == 2)
-      k_spread_mixed_zlanes<P><<<div_up(div_up(h->nsite, 32 / P) * 32, 128), 128, 0, h->stream>>>(
-          m, d_r, h->d_q, h->d_mask, h->nsite, h->d_mesh_fx);
-    else if (h->tune.spread_planes)
-      k_spread_mixed_planes<P><<<div_up(h->nsite * P, 128), 128, 0, h->stream>>>(m, d_r, h->d_q, h->d_mask,
-                                                                                  h->nsite, h->d_mesh_fx);
-    else
-      k_spread_mixed<P><<<div_up(h->nsite, 128), 128, 0, h->stream>>>(m, d_r, h->d_q, h->d_mask, h->nsite,
-                                                                       h->d_mesh_fx);
+    if (!(stage & 4))
+      spread_mixed_p<P>(h, m, d_r, 0, h->nsite);
     k_mesh_fx_to_f32<<<div_up((long) nr, 256), 256, 0, h->stream>>>(nr, h->d_mesh_fx, h->d_mesh32);
     timing_mark(h, "p3m_spread");
     if (cufftSetStream(h->plan_r2c32, h->stream) != CUFFT_SUCCESS ||
@@ -918,7 +935,7 @@ static cudaError_t p3m_mixed_p(mmnb_handle *h, const double *d_r, int stage)
     if (cufftExecC2R(h->plan_c2r32, h->d_meshk32, h->d_mesh32) != CUFFT_SUCCESS)
       return cudaErrorUnknown;
     timing_mark(h, "p3m_fft");
-    h->launches += 3;
+    h->launches += 2;
   }
   if (stage & 2) {
     if (h->d_egrid32)
@@ -930,6 +947,26 @@ static cudaError_t p3m_mixed_p(mmnb_handle *h, const double *d_r, int stage)
     h->launches += 1;
   }
   return cudaGetLastError();
+}
+
+template <int P>
+static cudaError_t spread_range_p(mmnb_handle *h, const double *d_r, int lo, int hi)
+{
+  spread_mixed_p<P>(h, mesh_args(h), d_r, lo, hi);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_spread_mixed_range(mmnb_handle *h, const double *d_r, int lo, int hi)
+{
+  switch (h->cfg.p3m_assignment_order) {
+  case 2: return spread_range_p<2>(h, d_r, lo, hi);
+  case 3: return spread_range_p<3>(h, d_r, lo, hi);
+  case 4: return spread_range_p<4>(h, d_r, lo, hi);
+  case 5: return spread_range_p<5>(h, d_r, lo, hi);
+  case 6: return spread_range_p<6>(h, d_r, lo, hi);
+  case 7: return spread_range_p<7>(h, d_r, lo, hi);
+  default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_p3m_mixed(mmnb_handle *h, const double *d_r, int stage)
