@@ -36,23 +36,31 @@ struct FinArgs {
   double *energy;
 };
 
+// sum over the block in a fixed order: lanes by a shuffle tree, then the
+// warps' sums in warp order (sh: one slot per warp plus one)
 __device__ __forceinline__ double block_sum(double v, double *sh)
 {
-  sh[threadIdx.x] = v;
+  constexpr int kWarps = kFinThreads / 32;
+  for (int o = 16; o > 0; o >>= 1)
+    v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0)
+    sh[threadIdx.x >> 5] = v;
   __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s)
-      sh[threadIdx.x] += sh[threadIdx.x + s];
-    __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < kWarps; w++)
+      t += sh[w];
+    sh[kWarps] = t;
   }
-  const double t = sh[0];
   __syncthreads();
+  const double t = sh[kWarps];
+  __syncthreads();  // sh may be reused at once
   return t;
 }
 
 __global__ void __launch_bounds__(kFinThreads) k_finalize(FinArgs a)
 {
-  __shared__ double se[kFinThreads];
+  __shared__ double se[kFinThreads / 32 + 1];
   __shared__ bool last;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double e = 0;
