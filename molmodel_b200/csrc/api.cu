@@ -1243,7 +1243,9 @@ static int compute_host(mmnb_handle *h, const double *r, double *f, double *u, m
       cudaError_t ce = cudaMemsetAsync(h->d_f, 0, sizeof(double) * n3, h->stream);
       if (ce == cudaSuccess)
         ce = cudaMemsetAsync(h->d_flags + kFlagOverflow, 0, sizeof(int), h->stream);
+      h->want_status = true;
       const int s = ce == cudaSuccess ? mmnb_compute_device(h, h->d_r, h->d_f, h->d_energy) : MMNB_ERR_CUDA;
+      h->want_status = false;
       h->capturing = false;
       h->in_chunks = false;
       cudaGraph_t g = nullptr;
@@ -1269,7 +1271,9 @@ static int compute_host(mmnb_handle *h, const double *r, double *f, double *u, m
       CK(cudaMemsetAsync(h->d_f, 0, sizeof(double) * n3, h->stream));
       CK(cudaMemsetAsync(h->d_flags + kFlagOverflow, 0, sizeof(int), h->stream));
       h->want_fields = phi || evec || keep;
+      h->want_status = true;
       const int s = mmnb_compute_device(h, h->d_r, h->d_f, h->d_energy);
+      h->want_status = false;
       h->want_fields = false;
       if (s)
         return s;

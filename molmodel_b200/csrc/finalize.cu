@@ -203,7 +203,7 @@ cudaError_t launch_finalize(mmnb_handle *h, double *d_f, double *d_energy)
   a.flags = h->d_flags;
   a.tail = h->cfg.include_lj_correction ? h->lj_correction : 0.0;
   a.energy = d_energy;
-  a.status = d_energy == h->d_energy ? h->d_status : nullptr;
+  a.status = h->want_status ? h->d_status : nullptr;
   k_finalize<<<h->elec_blocks, kFinThreads, 0, h->stream>>>(a);
   h->launches += 1;
   return cudaGetLastError();

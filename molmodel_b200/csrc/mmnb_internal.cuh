@@ -292,6 +292,8 @@ struct mmnb_handle {
   static constexpr int kStatusReady = 15;  // double slot of the ready word
   double *h_status = nullptr;
   double *d_status = nullptr;  // its device alias
+  bool want_status = false;    // set while the host call records its evaluation: no
+                               // other evaluation writes the block
   bool capturing = false;
 };
 

@@ -60,3 +60,32 @@ def test_host_call_with_the_ewald_sum_and_without_kspace():
             u = p.add_to_energy_and_forces(0.0, f, r)
             fresh = ElecLJ(precision="mixed", **cfg).init(wb).compute(r)
             assert np.array_equal(f, fresh["f"]) and u == fresh["total"]
+
+
+def test_host_call_after_an_asynchronous_device_evaluation():
+    """A device-array evaluation still in flight on the handle's stream (energy
+    left in the handle's own buffer) does not stand in for the host call that
+    follows it: the host call returns its own positions' energy and forces."""
+    import torch
+    wb = water_box(8, seed=13)
+    cfg = p3m(wb.box, 24)
+    p = ElecLJ(precision="mixed", **cfg).init(wb)
+    s = torch.cuda.Stream()
+    p.set_stream(s.cuda_stream)
+    rng = np.random.default_rng(7)
+    r1 = wb.positions + rng.normal(scale=0.03, size=wb.positions.shape)
+    r2 = wb.positions + rng.normal(scale=0.03, size=wb.positions.shape)
+    p.compute(r1)  # the host call's graph exists from here on
+    d_r = torch.tensor(r2.reshape(-1), dtype=torch.float64, device="cuda")
+    d_f = torch.zeros(3 * wb.nsite, dtype=torch.float64, device="cuda")
+    fresh = ElecLJ(precision="mixed", **cfg).init(wb).compute(r1)
+    other = ElecLJ(precision="mixed", **cfg).init(wb).compute(r2)
+    assert other["total"] != fresh["total"]
+    for _ in range(3):
+        for _ in range(4):
+            p.compute_device(d_r.data_ptr(), d_f.data_ptr(), 0)
+        f = np.zeros_like(r1)
+        u = p.add_to_energy_and_forces(0.0, f, r1)
+        assert u == fresh["total"]
+        assert np.array_equal(f, fresh["f"])
+    torch.cuda.synchronize()
