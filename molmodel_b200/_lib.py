@@ -62,7 +62,9 @@ SIGNATURES = [
     ("mmnb_create", ctypes.c_int, [ctypes.POINTER(MmnbConfig), ctypes.c_int, ctypes.c_int, _ip, ctypes.c_int, _ip,
                                    ctypes.c_int, _ip, ctypes.POINTER(_vp)]),
     ("mmnb_set_params", ctypes.c_int, [_vp, _ip, _dp, _dp, _dp, _dp]),
-    ("mmnb_compute", ctypes.c_int, [_vp, _dp, _dp, _dp, ctypes.POINTER(MmnbEnergy), _dp, _dp]),
+    # untyped pointers: the per-step host call passes raw addresses (typed
+    # pointer objects and byref() are accepted as well)
+    ("mmnb_compute", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("mmnb_compute_device", ctypes.c_int, [_vp, _vp, _vp, _vp]),
     ("mmnb_graph_capture", ctypes.c_int, [_vp, _vp, _vp, _vp]),
     ("mmnb_graph_launch", ctypes.c_int, [_vp]),

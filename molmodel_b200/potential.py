@@ -66,6 +66,7 @@ class ElecLJ:
         self.rebuild_interval = rebuild_interval
         self.device = device
         self._h = None
+        self._cells = None
         self.energy = None
 
     # ---- set-up --------------------------------------------------------------
@@ -179,10 +180,16 @@ class ElecLJ:
         lib = load()
         if f.dtype != np.float64 or not f.flags.c_contiguous:
             raise ValueError("f must be a C-contiguous float64 array")
-        r = np.ascontiguousarray(r, dtype=np.float64)
-        uu = ctypes.c_double(u)
-        e = MmnbEnergy()
-        check(lib.mmnb_compute(self._h, _d(r), _d(f), ctypes.byref(uu), ctypes.byref(e), None, None), self._h)
+        if not isinstance(r, np.ndarray) or r.dtype != np.float64 or not r.flags.c_contiguous:
+            r = np.ascontiguousarray(r, dtype=np.float64)
+        # per-call marshalling kept small (this is the per-step call): raw
+        # addresses and the potential's own energy and u cells
+        if self._cells is None:
+            self._cells = (ctypes.c_double(0.0), MmnbEnergy())
+        uu, e = self._cells
+        uu.value = u
+        check(lib.mmnb_compute(self._h, r.ctypes.data, f.ctypes.data, ctypes.addressof(uu), ctypes.addressof(e),
+                               None, None), self._h)
         self.energy = dict(elec=e.elec, lj=e.lj, lj_correction=e.lj_correction, total=e.total)
         return uu.value
 
