@@ -506,9 +506,9 @@ void free_all(mmnb_handle *h)
       cudaEventDestroy(ev);
       ev = nullptr;
     }
-  if (h->ev_flags) {
-    cudaEventDestroy(h->ev_flags);
-    h->ev_flags = nullptr;
+  if (h->ev_eval) {
+    cudaEventDestroy(h->ev_eval);
+    h->ev_eval = nullptr;
   }
   for (cudaEvent_t &ev : h->ev_in)
     if (ev) {
@@ -1200,8 +1200,8 @@ static int compute_host(mmnb_handle *h, const double *r, double *f, double *u, m
     return fail(h, MMNB_ERR_ARG, "null handle or positions");
   h->grad_ready = false;
   const size_t n3 = 3 * (size_t) h->nsite;
-  if (!h->ev_flags) {
-    CK(cudaEventCreateWithFlags(&h->ev_flags, cudaEventDisableTiming));
+  if (!h->ev_eval) {
+    CK(cudaEventCreateWithFlags(&h->ev_eval, cudaEventDisableTiming));
     for (cudaEvent_t &ev : h->ev_chunk)
       CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   }
@@ -1282,7 +1282,7 @@ static int compute_host(mmnb_handle *h, const double *r, double *f, double *u, m
     // overflow means evaluating again); the forces follow in chunks, each
     // added to f while the next one is in flight
     static_assert(4 + (kFlagCount + 1) / 2 <= mmnb_handle::kStatusReady, "status block");
-    CK(cudaEventRecord(h->ev_flags, h->stream));
+    CK(cudaEventRecord(h->ev_eval, h->stream));
     const int nch = mmnb_handle::kChunks;
     const size_t per = (n3 + nch - 1) / nch;
     for (int c = 0; c < nch; c++) {
@@ -1305,7 +1305,7 @@ static int compute_host(mmnb_handle *h, const double *r, double *f, double *u, m
     for (unsigned it = 1; *ready == 0ull; it++) {
       if ((it & 255u) != 0)
         continue;
-      const cudaError_t q = cudaEventQuery(h->ev_flags);
+      const cudaError_t q = cudaEventQuery(h->ev_eval);
       if (q == cudaErrorNotReady)
         continue;
       if (q != cudaSuccess)

@@ -275,7 +275,7 @@ struct mmnb_handle {
   // the host call copies the forces back in chunks and adds each as it lands
   static constexpr int kChunks = 2;
   cudaEvent_t ev_chunk[kChunks] = {};
-  cudaEvent_t ev_flags = nullptr;
+  cudaEvent_t ev_eval = nullptr;  // the host call's evaluation has ended (or failed)
   // ... and, replaying its graph, copies the positions in kInChunks pieces on
   // a stream of its own: the graph's mesh branch assigns the charges of each
   // piece as it lands (mixed form), everything else waits for the last piece
