@@ -399,6 +399,15 @@ static int grad_p3m_scratch(mmnb_handle *h, P3mScratch &s)
 
 using namespace mmnb;
 
+// dst[0, n) = src[0, n) on the host cores (the staging copies of a call)
+static void copy_host(double *dst, const double *src, size_t n)
+{
+  const long m = (long) n;
+#pragma omp parallel for schedule(static) if (m > (1 << 15))
+  for (long i = 0; i < m; i++)
+    dst[i] = src[i];
+}
+
 static int grad_fail(mmnb_handle *h, int code, const std::string &msg)
 {
   if (h)
@@ -423,7 +432,12 @@ extern "C" int mmnb_site_gradients(mmnb_handle *h, const double *dl_df, double *
       cudaFree(h->d_bwd);
     h->d_bwd = nullptr;
     h->bwd_cap = 0;
-    const cudaError_t ea = cudaMalloc(&h->d_bwd, need * sizeof(double));
+    if (h->h_bwd)
+      cudaFreeHost(h->h_bwd);
+    h->h_bwd = nullptr;
+    cudaError_t ea = cudaMalloc(&h->d_bwd, need * sizeof(double));
+    if (ea == cudaSuccess)
+      ea = cudaMallocHost((void **) &h->h_bwd, kGradSlots * n * sizeof(double));
     if (ea != cudaSuccess)
       return grad_fail(h, MMNB_ERR_CUDA, std::string("gradient scratch: ") + cudaGetErrorString(ea));
     h->bwd_cap = need;
@@ -477,8 +491,11 @@ extern "C" int mmnb_site_gradients(mmnb_handle *h, const double *dl_df, double *
   a.do14 = h->use_14 ? 1 : 0;
   a.out = d_out;
   cudaError_t e = cudaMemsetAsync(d_out, 0, sizeof(double) * kGradSlots * n, h->stream);
-  if (e == cudaSuccess && d_g)
-    e = cudaMemcpyAsync(d_g, dl_df, n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess && d_g) {
+    // through the handle's pinned force staging buffer (idle between host calls)
+    copy_host(h->h_f, dl_df, n3);
+    e = cudaMemcpyAsync(d_g, h->h_f, n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+  }
   if (e == cudaSuccess && h->cfg.include_rspace) {
     switch (h->G) {
     case 1: launch_grad_pair_g<1>(h, a); break;
@@ -505,13 +522,17 @@ extern "C" int mmnb_site_gradients(mmnb_handle *h, const double *dl_df, double *
   }
   double *outs[kGradSlots] = {du_dq, du_dsig, du_deps, dl_df ? dl_dq : nullptr, dl_df ? dl_dsig : nullptr,
                               dl_df ? dl_deps : nullptr};
-  for (int k = 0; k < kGradSlots && e == cudaSuccess; k++)
-    if (outs[k])
-      e = cudaMemcpyAsync(outs[k], d_out + k * n, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  // the slots are contiguous: one pinned copy back, then to the caller's arrays
+  const int nslot = dl_df ? kGradSlots : kDlDq;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h->h_bwd, d_out, nslot * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess)
     e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess)
     return grad_fail(h, MMNB_ERR_CUDA, std::string("site gradients: ") + cudaGetErrorString(e));
+  for (int k = 0; k < nslot; k++)
+    if (outs[k])
+      copy_host(outs[k], h->h_bwd + k * n, n);
   // LJ tail: U_tail = cA totA + cB totB over the classes' (sigma, eps, count);
   // d totA / d sig_i = 2 sum_b n_b dA_ab/dsig_a for site i in class a
   if (h->cfg.include_lj_correction && (du_dsig || du_deps) && !h->cls_sig.empty()) {

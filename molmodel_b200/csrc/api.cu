@@ -557,6 +557,8 @@ void free_all(mmnb_handle *h)
     cudaFreeHost(h->h_out);
   if (h->h_status)
     cudaFreeHost(h->h_status);
+  if (h->h_bwd)
+    cudaFreeHost(h->h_bwd);
   if (h->plan_r2c)
     cufftDestroy(h->plan_r2c);
   if (h->plan_c2r)

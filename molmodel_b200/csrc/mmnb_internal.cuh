@@ -208,6 +208,7 @@ struct mmnb_handle {
   // the dipole structure factor of the reciprocal sum
   double *d_bwd = nullptr;
   size_t bwd_cap = 0;
+  double *h_bwd = nullptr;  // pinned: the gradient slots come back in one copy
   bool grad_ready = false;           // the last evaluation was mmnb_forward's and nothing changed since
   // FP64 dipole solve for a mixed-form handle, which has no FP64 meshes or plans
   double *d_gmesh = nullptr;
