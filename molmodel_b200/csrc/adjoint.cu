@@ -40,6 +40,7 @@ namespace mmnb {
 
 constexpr int kGradWarps = 4;
 constexpr int kGradThreads = 128;
+constexpr int kGradQueue = 64;  // per warp: at most 31 carried over plus 32 new
 
 // per-site output slots of the scratch area (each nsite doubles)
 enum GradSlot { kDuDq = 0, kDuDsig, kDuDeps, kDlDq, kDlDsig, kDlDeps, kGradSlots };
@@ -93,49 +94,57 @@ __device__ __forceinline__ double3 load3(const double *p, int i)
   return make_double3(p[3 * i], p[3 * i + 1], p[3 * i + 2]);
 }
 
-// one warp per row (sorted group p); lanes walk the row's partners
+// One warp per row (sorted group p).  Lane l takes row site ia = l / P of the
+// group and partner slot l % P (P = 32 / G partners per step), so each lane
+// holds one row site's state.  The row's partners within rc are queued in list
+// order in a per-warp ring (the anchor test of 32 entries at a time); each step
+// evaluates P queued partners against every row site.  The row sites' sums are
+// reduced over the warp in a fixed order at the end.
 template <int G, bool SCREEN, bool GEXCL>
 __global__ void __launch_bounds__(kGradWarps * 32) k_grad_pair(GradArgs a)
 {
+  constexpr int P = 32 / G;
+  constexpr int kMask = kGradQueue - 1;
   const int lane = threadIdx.x & 31;
   const int p = blockIdx.x * kGradWarps + (threadIdx.x >> 5);
   if (p >= a.ngroup)
     return;  // the whole warp
   const int gi = a.sorted[p];
   const int si0 = a.group[2 * gi], ns = a.group[2 * gi + 1] - si0;
-  double4 ri[G];
-  double3 gv[G];
-  double sgi[G], epi[G], rsi[G];
-  int mi[G];
-  double psi[G], dus[G], due[G], dls[G], dle[G];
-#pragma unroll
-  for (int k = 0; k < G; k++) {
-    psi[k] = dus[k] = due[k] = dls[k] = dle[k] = 0;
-    mi[k] = 0;
-    ri[k] = make_double4(0, 0, 0, 0);
-    gv[k] = make_double3(0, 0, 0);
-    sgi[k] = epi[k] = rsi[k] = 0;
-    if (k < ns) {
-      const int s = si0 + k;
-      ri[k] = make_double4(a.r[3 * s], a.r[3 * s + 1], a.r[3 * s + 2], a.q[s]);
-      if (a.g)
-        gv[k] = load3(a.g, s);
-      sgi[k] = a.sig[s];
-      epi[k] = a.eps[s];
-      rsi[k] = a.rscreen[s];
-      mi[k] = a.mask[s];
-    }
+  const int ia = lane / P, pk = lane % P;
+  const bool act = ia < G && ia < ns;
+  // the row's anchor (the minimum image is taken between anchors) and this
+  // lane's row site
+  const double4 r0 = make_double4(a.r[3 * si0], a.r[3 * si0 + 1], a.r[3 * si0 + 2], 0);
+  const double3 g0 = a.g ? load3(a.g, si0) : make_double3(0, 0, 0);
+  double4 ri = make_double4(0, 0, 0, 0);
+  double3 gv = make_double3(0, 0, 0);
+  double sgi = 0, epi = 0, rsi = 0;
+  int mi = 0;
+  if (act) {
+    const int s = si0 + ia;
+    ri = make_double4(a.r[3 * s], a.r[3 * s + 1], a.r[3 * s + 2], a.q[s]);
+    if (a.g)
+      gv = load3(a.g, s);
+    sgi = a.sig[s];
+    epi = a.eps[s];
+    rsi = a.rscreen[s];
+    mi = a.mask[s];
   }
+  double psi = 0, dus = 0, due = 0, dls = 0, dle = 0;
   const int cnt = a.nbr_count[p];
   const int *row = a.nbr + (size_t) p * a.rowcap;
-  for (int e = lane; e < cnt; e += 32) {
-    const int gj = a.sorted[row[e]];
+  __shared__ double qd[kGradWarps][7][kGradQueue];
+  __shared__ int qg[kGradWarps][kGradQueue];
+  double(*wq)[kGradQueue] = qd[threadIdx.x >> 5];
+  int *wg = qg[threadIdx.x >> 5];
+  const unsigned below = (1u << lane) - 1;
+  // row site ia against the queued partner in ring slot k
+  auto partner = [&](int k) {
+    const int gj = wg[k];
+    const double x = wq[0][k], y = wq[1][k], z = wq[2][k], sx = wq[3][k], sy = wq[4][k], sz = wq[5][k];
+    const double r2a = wq[6][k];
     const int sj0 = a.group[2 * gj], nsj = a.group[2 * gj + 1] - sj0;
-    const double4 rjA = make_double4(a.r[3 * sj0], a.r[3 * sj0 + 1], a.r[3 * sj0 + 2], 0);
-    double x, y, z, sx, sy, sz;
-    const double r2a = anchor_disp(a.box, ri[0], rjA, x, y, z, sx, sy, sz);
-    if (r2a > a.rhi2)
-      continue;
     double S = 1, ds = 0;
     if (r2a > a.rlo2) {
       const double zz = (r2a - a.rlo2) * a.inv_sw;
@@ -145,7 +154,7 @@ __global__ void __launch_bounds__(kGradWarps * 32) k_grad_pair(GradArgs a)
     double GR = 0;
     if (a.g && ds != 0) {
       const double3 gB = load3(a.g, sj0);
-      GR = (gv[0].x - gB.x) * x + (gv[0].y - gB.y) * y + (gv[0].z - gB.z) * z;
+      GR = (g0.x - gB.x) * x + (g0.y - gB.y) * y + (g0.z - gB.z) * z;
     }
     bool gx = false;
     if (GEXCL)
@@ -155,77 +164,104 @@ __global__ void __launch_bounds__(kGradWarps * 32) k_grad_pair(GradArgs a)
       if (jb >= nsj)
         break;
       const int sj = sj0 + jb;
-      const int mj = a.mask[sj];
+      const int m = mi & a.mask[sj];
+      if (!m)
+        continue;
+      if (GEXCL && gx && csr_has(a.excl_ptr, a.excl_idx, si0 + ia, sj))
+        continue;
       const double xj = a.r[3 * sj], yj = a.r[3 * sj + 1], zj = a.r[3 * sj + 2];
-      const double qj = a.q[sj];
       const double3 gj3 = a.g ? load3(a.g, sj) : make_double3(0, 0, 0);
-#pragma unroll
-      for (int ia = 0; ia < G; ia++) {
-        const int m = mi[ia] & mj;
-        if (!m)
-          continue;
-        if (GEXCL && gx && csr_has(a.excl_ptr, a.excl_idx, si0 + ia, sj))
-          continue;
-        double dx, dy, dz, r2;
-        if (ia == 0 && jb == 0) {
-          dx = x;
-          dy = y;
-          dz = z;
-          r2 = r2a;
-        } else {
-          dx = (ri[ia].x + sx) - xj;
-          dy = (ri[ia].y + sy) - yj;
-          dz = (ri[ia].z + sz) - zj;
-          r2 = dx * dx + dy * dy + dz * dz;
-        }
-        if (m & MMNB_SITE_HAS_Q) {
-          double b0, b1, fseg;
-          int seg;
-          ewald_table_b(a.cheb, a.cheb_min, a.cheb_max, a.cheb_inv_dx, a.eta, r2, b0, b1, seg, fseg);
-          if (SCREEN) {
-            const double rs = rsi[ia] + a.rscreen[sj];
-            if (r2 < rs * rs) {
-              const double invr = 1.0 / sqrt(r2);
-              const double inv3 = 1.0 / (rs * rs * rs);
-              b0 += (-0.5 * r2 * inv3 + 1.5 / rs) - invr;
-              b1 += inv3 - invr * invr * invr;
-            }
+      double dx, dy, dz, r2;
+      if (ia == 0 && jb == 0) {
+        dx = x;
+        dy = y;
+        dz = z;
+        r2 = r2a;
+      } else {
+        dx = (ri.x + sx) - xj;
+        dy = (ri.y + sy) - yj;
+        dz = (ri.z + sz) - zj;
+        r2 = dx * dx + dy * dy + dz * dz;
+      }
+      if (m & MMNB_SITE_HAS_Q) {
+        double b0, b1, fseg;
+        int seg;
+        ewald_table_b(a.cheb, a.cheb_min, a.cheb_max, a.cheb_inv_dx, a.eta, r2, b0, b1, seg, fseg);
+        if (SCREEN) {
+          const double rs = rsi + a.rscreen[sj];
+          if (r2 < rs * rs) {
+            const double invr = 1.0 / sqrt(r2);
+            const double inv3 = 1.0 / (rs * rs * rs);
+            b0 += (-0.5 * r2 * inv3 + 1.5 / rs) - invr;
+            b1 += inv3 - invr * invr * invr;
           }
-          const double gjd = gj3.x * dx + gj3.y * dy + gj3.z * dz;
-          psi[ia] += qj * (ds * GR * b0 - S * b1 * gjd);
         }
-        if (m & MMNB_SITE_HAS_LJ) {
-          const LJd t = lj_terms(sgi[ia], a.sig[sj], epi[ia], a.eps[sj], a.geometric, r2);
-          const double gd = (gv[ia].x - gj3.x) * dx + (gv[ia].y - gj3.y) * dy + (gv[ia].z - gj3.z) * dz;
-          dus[ia] += S * t.us;
-          due[ia] += S * t.u;
-          dls[ia] += S * t.dus * gd + ds * GR * t.us;
-          dle[ia] += S * t.du * gd + ds * GR * t.u;
-        }
+        const double gjd = gj3.x * dx + gj3.y * dy + gj3.z * dz;
+        psi += a.q[sj] * (ds * GR * b0 - S * b1 * gjd);
+      }
+      if (m & MMNB_SITE_HAS_LJ) {
+        const LJd t = lj_terms(sgi, a.sig[sj], epi, a.eps[sj], a.geometric, r2);
+        const double gd = (gv.x - gj3.x) * dx + (gv.y - gj3.y) * dy + (gv.z - gj3.z) * dz;
+        dus += S * t.us;
+        due += S * t.u;
+        dls += S * t.dus * gd + ds * GR * t.us;
+        dle += S * t.du * gd + ds * GR * t.u;
       }
     }
-  }
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-#pragma unroll
-    for (int k = 0; k < G; k++) {
-      psi[k] += __shfl_xor_sync(0xffffffffu, psi[k], off);
-      dus[k] += __shfl_xor_sync(0xffffffffu, dus[k], off);
-      due[k] += __shfl_xor_sync(0xffffffffu, due[k], off);
-      dls[k] += __shfl_xor_sync(0xffffffffu, dls[k], off);
-      dle[k] += __shfl_xor_sync(0xffffffffu, dle[k], off);
+  };
+  int head = 0, qn = 0;  // ring entries [head, head + qn)
+  for (int base = 0; base < cnt; base += 32) {
+    const int e = base + lane;
+    bool take = false;
+    double x = 0, y = 0, z = 0, sx = 0, sy = 0, sz = 0, r2a = 0;
+    int gj = 0;
+    if (e < cnt) {
+      gj = a.sorted[row[e]];
+      const int sj0 = a.group[2 * gj];
+      const double4 rjA = make_double4(a.r[3 * sj0], a.r[3 * sj0 + 1], a.r[3 * sj0 + 2], 0);
+      r2a = anchor_disp(a.box, r0, rjA, x, y, z, sx, sy, sz);
+      take = r2a <= a.rhi2;
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, take);
+    if (take) {
+      const int k = (head + qn + __popc(bal & below)) & kMask;
+      wq[0][k] = x;
+      wq[1][k] = y;
+      wq[2][k] = z;
+      wq[3][k] = sx;
+      wq[4][k] = sy;
+      wq[5][k] = sz;
+      wq[6][k] = r2a;
+      wg[k] = gj;
+    }
+    qn += __popc(bal);
+    __syncwarp();
+    for (; qn >= P; qn -= P, head = (head + P) & kMask) {
+      if (act)
+        partner((head + pk) & kMask);
+      __syncwarp();  // the slots are free again only after every lane has read them
     }
   }
+  if (act && pk < qn)
+    partner((head + pk) & kMask);
+  // each row site's sums over its lanes (the other lanes add zero), in a fixed order
   const size_t n = a.nsite;
 #pragma unroll
-  for (int k = 0; k < G; k++) {
-    if (lane == k && k < ns) {
-      const int s = si0 + k;
-      a.out[kDlDq * n + s] += psi[k];
-      a.out[kDuDsig * n + s] += dus[k];
-      a.out[kDuDeps * n + s] += due[k];
-      a.out[kDlDsig * n + s] += dls[k];
-      a.out[kDlDeps * n + s] += dle[k];
+  for (int t = 0; t < G; t++) {
+    double v[5] = {ia == t ? psi : 0.0, ia == t ? dus : 0.0, ia == t ? due : 0.0, ia == t ? dls : 0.0,
+                   ia == t ? dle : 0.0};
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+      for (int c = 0; c < 5; c++)
+        v[c] += __shfl_xor_sync(0xffffffffu, v[c], off);
+    if (lane == 0 && t < ns) {
+      const int s = si0 + t;
+      a.out[kDlDq * n + s] += v[0];
+      a.out[kDuDsig * n + s] += v[1];
+      a.out[kDuDeps * n + s] += v[2];
+      a.out[kDlDsig * n + s] += v[3];
+      a.out[kDlDeps * n + s] += v[4];
     }
   }
 }
