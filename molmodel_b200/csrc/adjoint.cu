@@ -51,6 +51,10 @@ struct GradArgs {
   double rlo2, rhi2, inv_sw, eta;
   double cheb_min, cheb_max, cheb_inv_dx;
   const double *cheb;
+  // the rigid-water forward's copy of the table: the cubics' (c0, c1) and
+  // (c2, c3), continued to (rc + 2.5)^2 (k_grad_pair)
+  const double2 *tw0, *tw1;
+  double nsegw;
   const double *r, *q, *sig, *eps, *rscreen;
   const double *g;  // dL/dF, 3 per site, or null
   const int *mask, *nbr, *nbr_count, *sorted, *group;
@@ -87,6 +91,27 @@ __device__ __forceinline__ LJd lj_terms(double si, double sj, double ei, double 
   t.us = kap * (2 * a12 - b6);
   t.dus = kap * (24 * a12 - 6 * b6) * ir2;
   return t;
+}
+
+// b0 = erfc(eta r)/r from the table's cubic and b1 = -(2 / dx) d b0/d(segment
+// position) from its derivative: the reference stores b1's quadratic as
+// exactly that derivative (-2 k c_k / dx, k = 1..3), so half the table is
+// read; outside the table the exact functions
+__device__ __forceinline__ void ewald_grad_b(const GradArgs &a, double r2, double &b0, double &b1)
+{
+  const double x = (r2 - a.cheb_min) * a.cheb_inv_dx;
+  if (x > 0 && x < a.nsegw) {
+    const int i = (int) x;
+    const double f = x - i;
+    const double2 c01 = __ldg(a.tw0 + i), c23 = __ldg(a.tw1 + i);
+    b0 = ((c23.y * f + c23.x) * f + c01.y) * f + c01.x;
+    b1 = -2 * a.cheb_inv_dx * ((3 * c23.y * f + 2 * c23.x) * f + c01.y);
+  } else {
+    const double r = sqrt(r2);
+    const double er = a.eta * r;
+    b0 = erfc(er) / r;
+    b1 = (b0 + a.eta * M_2_SQRTPI * exp(-(er * er))) / r2;
+  }
 }
 
 __device__ __forceinline__ double3 load3(const double *p, int i)
@@ -184,9 +209,8 @@ __global__ void __launch_bounds__(kGradWarps * 32) k_grad_pair(GradArgs a)
         r2 = dx * dx + dy * dy + dz * dz;
       }
       if (m & MMNB_SITE_HAS_Q) {
-        double b0, b1, fseg;
-        int seg;
-        ewald_table_b(a.cheb, a.cheb_min, a.cheb_max, a.cheb_inv_dx, a.eta, r2, b0, b1, seg, fseg);
+        double b0, b1;
+        ewald_grad_b(a, r2, b0, b1);
         if (SCREEN) {
           const double rs = rsi + a.rscreen[sj];
           if (r2 < rs * rs) {
@@ -501,6 +525,9 @@ extern "C" int mmnb_site_gradients(mmnb_handle *h, const double *dl_df, double *
   a.cheb_max = h->cheb_max;
   a.cheb_inv_dx = h->cheb_inv_dx;
   a.cheb = h->d_cheb;
+  a.tw0 = reinterpret_cast<const double2 *>(h->d_cheb_w);
+  a.tw1 = a.tw0 + h->cheb_w_nseg;
+  a.nsegw = h->cheb_w_nseg;
   a.r = h->d_r;  // the forward's positions (host path)
   a.q = h->d_q;
   a.sig = h->d_sig;
