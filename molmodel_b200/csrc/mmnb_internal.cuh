@@ -398,6 +398,35 @@ __device__ __forceinline__ void ewald_table_b(const double *cheb, double cmin, d
   }
 }
 
+// The same from the cubic alone: t0[i] = (c0, c1), t1[i] = (c2, c3) of segment i
+// (the rigid-water kernels' copy of the table, whose first 512 segments are the
+// reference's), b1 from the cubic's derivative -- the reference stores b1's
+// quadratic as exactly -2 k c_k / dx (k = 1..3), so the two differ only in
+// rounding.  Same range, segment and position as ewald_table_b; half the reads.
+__device__ __forceinline__ void ewald_table_half(const double2 *t0, const double2 *t1, double cmin, double cmax,
+                                                 double inv_dx, double eta, double r2, double &b0, double &b1,
+                                                 int &seg, double &f)
+{
+  if (cmin < r2 && r2 < cmax) {
+    double x = (r2 - cmin) * inv_dx;
+    const unsigned i = (unsigned) x;
+    const double2 c01 = __ldg(t0 + i), c23 = __ldg(t1 + i);
+    x -= i;
+    b0 = ((c23.y * x + c23.x) * x + c01.y) * x + c01.x;
+    b1 = -2 * inv_dx * ((3 * c23.y * x + 2 * c23.x) * x + c01.y);
+    seg = (int) i;
+    f = x;
+  } else {
+    const double r = sqrt(r2);
+    const double er = eta * r;
+    const double e = exp(-(er * er));
+    b0 = erfc(er) / r;
+    b1 = (b0 + eta * M_2_SQRTPI * e) / r2;
+    seg = -1;
+    f = 0;
+  }
+}
+
 // minimum image of one site displacement, rounded as the reference rounds it
 __device__ __forceinline__ void min_image_ref(const Box &b, double &x, double &y, double &z)
 {

@@ -45,13 +45,14 @@ struct PairArgs {
   double *phi, *evec, *ljf, *lj_part;
   double *vir_part;  // per block: sum of the virial's pair term (mmnb_virial), or null
   const double *cheb_d;  // 512 x 4: cubics of -eta d/d(eta) of the table (mmnb_virial)
+  const double2 *tw0, *tw1;  // the table's cubics: (c0, c1) and (c2, c3) per segment
 };
 
 // b0 = erfc(eta r)/r, b1 = (b0 + 2 eta/sqrt(pi) exp(-eta^2 r^2)) / r^2; seg and
 // f: the table segment and the position in it (seg = -1 outside the table)
 __device__ __forceinline__ void ewald_b(const PairArgs &a, double r2, double &b0, double &b1, int &seg, double &f)
 {
-  ewald_table_b(a.cheb, a.cheb_min, a.cheb_max, a.cheb_inv_dx, a.eta, r2, b0, b1, seg, f);
+  ewald_table_half(a.tw0, a.tw1, a.cheb_min, a.cheb_max, a.cheb_inv_dx, a.eta, r2, b0, b1, seg, f);
 }
 
 // The table is refitted for each eta, so along the volume-move path its eta
@@ -517,6 +518,8 @@ cudaError_t launch_rspace_fp64(mmnb_handle *h)
   a.lj_part = h->d_lj_part;
   a.vir_part = h->want_virial ? h->d_vir_part : nullptr;
   a.cheb_d = h->d_cheb_d;
+  a.tw0 = reinterpret_cast<const double2 *>(h->d_cheb_w);
+  a.tw1 = a.tw0 + h->cheb_w_nseg;
   switch (h->G) {
   case 1: launch_pair_g<1>(h, a); break;
   case 2: launch_pair_g<2>(h, a); break;
